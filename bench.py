@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 gravity path: particle-steps/s of the full step.
+
+A step is one pass of the hot path over the whole galaxy: Morton codes, sort,
+gather, BFS octree build, COM refresh, Barnes-Hut walk + halo + kick-drift
+(+ star formation), replayed from a CUDA graph. Default workload: the single
+disk of N = 524288 (30% gas, star formation, eps 0.02, theta 0.5, dt 0.005).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank runs an independent replica
+(the path does not shard; there is no collective): weak scaling, value = all
+ranks' particle-steps / the slowest rank's device time.
+
+Timing: W untimed warm-up steps, then K steps, each bracketed by CUDA events on
+the context's stream, with a 256 MiB L2 flush (2x the 126 MB L2) between steps;
+barrier + synchronize on both sides; max over ranks. ``e2e`` is the same
+metric through the C ABI with pinned host buffers: upload of the initial
+state, per step a Params upload and an energy-diagnostic readback, and a final
+state readback, all inside the event-timed region.
+
+``--impl reference`` times the reference algorithm on the host cores: the CPU
+restatement in oracle/ (sort + build single-threaded like the reference's Web
+Worker, refresh + walk + kick-drift on all cores), each step a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s (full sort+build+refresh+walk+integrate step)"
+UNIT = "particle-steps/s"
+FLOPS_PER_INTERACTION = 23
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="disk512k")
+    ap.add_argument("--theta", type=float, default=None)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def init_dist(ws, backend):
+    if ws <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def workload(args):
+    from galaxy_sim_b200 import simulation as S
+
+    w = S.WORKLOADS[args.workload]
+    if args.theta is not None:
+        w = S.with_theta(w, args.theta)
+    return w
+
+
+def config_of(w, g, args, l2="flush 256 MiB between timed steps"):
+    ph = w.physics
+    return {"workload": w.name, "N": int(g.N), "theta": ph.theta, "epsilon": ph.epsilon,
+            "dt": ph.dt, "gas_drag": ph.gas_drag, "sf_eff": ph.sf_eff, "bucket": 16,
+            "morton_bits": 30, "precision": "fp32 walk, fp32 COM refresh",
+            "parallelism": f"replicas x{args.gpus} (no collective)", "l2": l2}
+
+
+class Clocks:
+    """nvidia-smi sampler during the timed region (median SM MHz under load, reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,utilization.gpu,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(self.index), "-lms", "100"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 10:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), float(parts[4]), parts[6:10]))
+            except ValueError:
+                continue
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        load = [r for r in rows if r[2] > 10] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in load for k in range(4) if r[3][k].lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in load), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(load)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+def run_ours(args, ws, rank, local):
+    import numpy as np
+    import torch
+
+    from galaxy_sim_b200 import _lib
+    from galaxy_sim_b200.simulation import Simulation, params_dict
+
+    torch.cuda.set_device(local)
+    dist = init_dist(ws, "nccl")
+    w = workload(args)
+    g = w.make()
+    N = g.N
+    sim = Simulation(g, w.physics, device=local)
+    ext = torch.cuda.ExternalStream(sim.gpu.stream, device=torch.device("cuda", local))
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+    # kernels per step: bbox, codes, 4 sort passes, gather, 4 build kernels, walk (+SF fused)
+    n_launch_step = 12
+
+    sim.run(args.warmup)
+    sim.sync()
+    K = args.steps
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        for k in range(K):
+            with torch.cuda.stream(ext):
+                flush.fill_(float(k))          # evict the previous step from L2 (untimed)
+                starts[k].record(ext)
+            sim.run(1)
+            with torch.cuda.stream(ext):
+                ends[k].record(ext)
+        sim.sync()
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    errs = sim.gpu.deviceErrors()
+    if errs:
+        raise RuntimeError(f"device error word 0x{errs:x} during the timed steps")
+    t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = N * K * ws / (max_ms / 1e3)
+    clocks = clk.summary()
+
+    # ---- walk kernel, timed alone on the same stream (roofline of the dominant kernel) ----
+    sim.gpu.setDebug(True)
+    sim.gpu.counters(reset=True)
+    sim.gpu.sortBuild()
+    sim.gpu.step()
+    cnt = sim.gpu.counters(reset=True)
+    sim.gpu.setDebug(False)
+    interactions = cnt[0] + cnt[1]
+    R = 10
+    walk_ms, build_ms = [], []
+    for _ in range(R):
+        a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        with torch.cuda.stream(ext):
+            flush.fill_(1.0)
+            a.record(ext)
+        sim.gpu.sortBuild()
+        with torch.cuda.stream(ext):
+            b.record(ext)
+        sim.gpu.step()
+        with torch.cuda.stream(ext):
+            c.record(ext)
+        sim.sync()
+        build_ms.append(a.elapsed_time(b))
+        walk_ms.append(b.elapsed_time(c))
+    walk_avg = sum(walk_ms) / R
+    fp32_peak = 148 * 128 * 2 * float(measured_peaks().get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
+    achieved = interactions * FLOPS_PER_INTERACTION / (walk_avg / 1e3) / 1e12
+    roofline = {"kernel": "walk_kernel (BH walk + halo + kick-drift)", "bound": "fp32",
+                "achieved": round(achieved, 3), "peak": round(fp32_peak, 2), "unit": "TFLOP/s",
+                "frac": round(achieved / fp32_peak, 4),
+                "peak_source": "nominal FP32 pipe: 148 SM x 128 lanes x 2 x sm_max_mhz "
+                               "(MEASURED_PEAKS.json holds no FP32 figure)",
+                "algorithmic": f"{interactions / N:.1f} interactions/particle x {N} particles x "
+                               f"{FLOPS_PER_INTERACTION} flops per launch",
+                "walk_ms": round(walk_avg, 4), "sort_build_refresh_ms": round(sum(build_ms) / R, 4),
+                "traffic": None}
+
+    # ---- e2e through the C ABI with pinned host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        import ctypes as C
+
+        L = _lib.lib()
+        hp = torch.from_numpy(g.particles.reshape(-1)).pin_memory()
+        hs = torch.from_numpy(g.stellar.reshape(-1)).pin_memory()
+        outp = torch.empty(N * 8, dtype=torch.float32).pin_memory()
+        outs = torch.empty(N * 4, dtype=torch.float32).pin_memory()
+        prm = _lib.GsParams()
+        pd = params_dict(g, w.physics)
+        sim.gpu.updateParams(**pd)
+        prm = sim.gpu._params
+        diag = _lib.GsDiag()
+        ctx = sim.gpu._ctx
+        Ke = K
+        sim.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(ext):
+            e0.record(ext)
+        _lib.check(L.gs_write_state(ctx, hp.data_ptr(), hs.data_ptr()), ctx)
+        for k in range(Ke):
+            prm.time = k * w.physics.dt   # main.js passes simTime with every updateParams
+            _lib.check(L.gs_update_params(ctx, C.byref(prm)), ctx)
+            _lib.check(L.gs_run(ctx, 1, int(sim.star_formation)), ctx)
+            _lib.check(L.gs_energy(ctx, C.byref(diag)), ctx)
+        _lib.check(L.gs_read_state(ctx, outp.data_ptr(), outs.data_ptr()), ctx)
+        with torch.cuda.stream(ext):
+            e1.record(ext)
+        torch.cuda.synchronize()
+        te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f"cuda:{local}")
+        if dist:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        te_ms = float(te.item())
+        if not np.isfinite(diag.e_diag):
+            raise RuntimeError("non-finite energy diagnostic in the e2e run")
+        e2e = {"value": round(N * Ke * ws / (te_ms / 1e3), 1), "unit": UNIT,
+               "h2d_bytes_per_step": int(round((N * 48 + Ke * 96) / Ke)),
+               "d2h_bytes_per_step": int(round((Ke * 48 + N * 48) / Ke)),
+               "path": "gs_write_state (pinned) + K x [gs_update_params, gs_run(1), gs_energy] "
+                       "+ gs_read_state (pinned)", "steps": Ke, "ms": round(te_ms, 3)}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline(w, g, steps=5, warmup=1, budget_s=15.0)
+    sim.close()
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    step_sorted = sorted(step_ms)
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": ws, "steps": K,
+        "warmup": args.warmup, "ms_per_step": round(max_ms / K, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ICs)",
+        "config": config_of(w, g, args),
+        "latency_ms": {"p50": round(step_sorted[len(step_sorted) // 2], 5),
+                       "p99": round(step_sorted[min(len(step_sorted) - 1, int(0.99 * len(step_sorted)))], 5),
+                       "max": round(step_sorted[-1], 5)},
+        "interactions_per_particle": round(interactions / N, 2),
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+        "gpu_launches": K * n_launch_step,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(w, g, steps, warmup, budget_s, nthreads=0):
+    """The oracle's full step on the host cores (a bounded sample of the workload).
+
+    Every step runs the complete codes + sort + build (one thread, like the
+    reference's Web Worker) and refresh; the walk + kick-drift runs on all
+    threads for every stride-th particle, stride chosen so that warmup + steps
+    fit the time budget, and its time is scaled by the stride.
+    """
+    import numpy as np
+
+    import oracle as O
+    from galaxy_sim_b200.simulation import params_dict
+
+    O.build()
+    pd = params_dict(g, w.physics)
+    hc = pd.pop("haloCenters")
+    p = O.make_params(g.N, haloCenters=[c[:3] for c in hc], **pd)
+    pl = O.Pipeline(g.particles, g.stellar, p, central=g.central, halo_centers=[c[:3] for c in hc],
+                    nthreads=nthreads)
+    sf = w.physics.sf_eff > 0
+    pl.step(sf, 64)                              # probe: build time + 1/64 of the walk
+    t_build, walk_full = pl.t_build, pl.t_walk * 64
+    per_step = budget_s / max(1, steps + warmup)
+    stride = max(1, int(np.ceil(walk_full / max(per_step - t_build, 0.02))))
+    for _ in range(warmup):
+        pl.step(sf, stride)
+    pl.t_build = pl.t_walk = 0.0
+    for _ in range(steps):
+        pl.step(sf, stride)
+    est_step = (pl.t_build + pl.t_walk * stride) / steps
+    cores = nthreads or os.cpu_count()
+    return {"value": round(g.N / est_step, 1), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{steps} timed steps (+{warmup} warm-up) of {w.name} (N={g.N}): codes+sort+"
+                      f"build+refresh on 1 thread (like the reference's Web Worker), walk+integrate "
+                      f"of every {stride}-th particle on {cores} threads, walk time scaled x{stride}",
+            "build_s_per_step": round(pl.t_build / steps, 4),
+            "walk_s_per_step_est": round(pl.t_walk * stride / steps, 4)}
+
+
+def run_reference(args, ws, rank, local):
+    if rank != 0:
+        return
+    w = workload(args)
+    g = w.make()
+    cpu = cpu_baseline(w, g, steps=args.steps, warmup=args.warmup, budget_s=150.0)
+    line = {
+        "metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * g.N / cpu["value"], 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded ICs)", "impl": "reference",
+        "config": config_of(w, g, args, l2="host run"),
+        "cpu_baseline": cpu,
+        "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, ws, rank, local)
+    else:
+        run_ours(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,441 @@
+// Breadth-first bucketed octree on the device, bit-exact with MortonTree.build
+// (src/physics/mortonTree.js:107-182), without level-synchronous launches.
+//
+// For sorted 30-bit codes c[0..N), let cpd(a, b) be the number of leading
+// 3-bit digits a and b share (10 if equal). The reference's BFS has these
+// closed forms, which the kernels below evaluate per particle:
+//   * particle i starts a new depth-d group iff d >= D(i), with D(0) = 0 and
+//     D(i) = cpd(c[i-1], c[i]) + 1 (11 = never);
+//   * the depth-d group of i holds > 16 particles iff some j in [i-16, i] with
+//     j + 16 < N has cpd(c[j], c[j+16]) >= d (sorted codes: a run of 17 equal
+//     prefixes), so with M(i) = max of those cpd (or -1), the node of i at depth
+//     d is internal iff d < min(10, M(i) + 1) =: L(i), its leaf depth
+//     (count <= BUCKET || depth >= MAX_LEVEL, mortonTree.js:126);
+//   * i therefore starts exactly the nodes at depths D(i)..L(i); BFS numbers
+//     the nodes of a level in queue order, which is prefix order, so node
+//     (d, i) has index levelStart(d) + #{j < i : D(j) <= d <= L(j)}.
+// The third leaf clause of mortonTree.js:127 (numNodes + 8 > maxNodes) cannot
+// fire for the reference's pool of 2N + 4096 nodes: a tree has at most N leaves
+// and at most 10 * N / 17 internal nodes. The kernels flag a pool where it could.
+#pragma once
+#include "common.cuh"
+#include "morton.cuh"
+
+namespace gs {
+
+constexpr int kFlagThreads = 256;
+constexpr int kFlagPer = 4;                          // consecutive particles per thread
+constexpr int kFlagTile = kFlagThreads * kFlagPer;   // 1024 particles per block
+constexpr int kCounters = 12;                        // depths 0..10 + leaf starts
+
+// cpd of two codes: leading equal 3-bit digits (0..10).
+__device__ inline int cpd(uint32_t a, uint32_t b) {
+  const uint32_t x = a ^ b;
+  if (x == 0) return 10;
+  const int msb = 31 - __clz(x);  // 0..29 for 30-bit codes
+  return (29 - msb) / 3;
+}
+
+struct BuildBuffers {
+  const uint32_t* codes;  // sorted codes [N]
+  uint32_t N;
+  uint32_t cap;           // node pool size
+  uint32_t max_nodes;     // MortonTree pool whose third leaf clause is checked
+  uint8_t* dl;            // packed D | L << 4 per particle [N]
+  uint32_t* blk_counts;   // [blocks][12]
+  uint32_t* blk_offs;     // [blocks][12]
+  TreeMeta* meta;
+  uint32_t* node_start;   // [cap]
+  uint32_t* child_base;   // [cap]
+  int32_t* parent;        // [cap]
+  uint8_t* depth;         // [cap]
+  uint32_t* arrive;       // [cap], zero between builds
+  uint32_t* leaf_node;    // [N + 1]
+  uint32_t* leaf_start;   // [N + 1]
+  float4* cm;             // [cap] com.xyz, mass
+  WalkInfo* info;         // [cap]
+};
+
+// K1: per particle D, L and per-block start counts.
+__global__ void __launch_bounds__(kFlagThreads) tree_flags_kernel(BuildBuffers b, DevState* st) {
+  __shared__ uint32_t s_code[kFlagTile + 32];
+  __shared__ int8_t s_cpd16[kFlagTile + 16];
+  __shared__ uint32_t s_red[kFlagThreads / 32][kCounters];
+  const int tid = threadIdx.x;
+  const int64_t base = (int64_t)blockIdx.x * kFlagTile;
+  const uint32_t N = b.N;
+  if (st && blockIdx.x == 0 && tid < 2) st->central[tid] = st->central_next[tid];
+  // codes [base-16, base+tile+16)
+  for (int k = tid; k < kFlagTile + 32; k += kFlagThreads) {
+    const int64_t g = base - 16 + k;
+    s_code[k] = (g >= 0 && g < N) ? b.codes[g] : 0u;
+  }
+  __syncthreads();
+  // cpd16(j) for j in [base-16, base+tile): -1 when j < 0 or j + 16 >= N
+  for (int k = tid; k < kFlagTile + 16; k += kFlagThreads) {
+    const int64_t j = base - 16 + k;
+    s_cpd16[k] = (j >= 0 && j + 16 < (int64_t)N) ? (int8_t)cpd(s_code[k], s_code[k + 16]) : (int8_t)-1;
+  }
+  __syncthreads();
+  uint32_t cnt[kCounters];
+#pragma unroll
+  for (int k = 0; k < kCounters; k++) cnt[k] = 0;
+  uint32_t packed = 0;
+#pragma unroll
+  for (int q = 0; q < kFlagPer; q++) {
+    const int loc = tid * kFlagPer + q;
+    const int64_t i = base + loc;
+    if (i >= N) break;
+    int D;
+    if (i == 0) {
+      D = 0;
+    } else {
+      const uint32_t a = s_code[loc + 15], c = s_code[loc + 16];
+      D = (a == c) ? 11 : cpd(a, c) + 1;
+    }
+    int M = -1;
+#pragma unroll
+    for (int w = 0; w <= 16; w++) M = max(M, (int)s_cpd16[loc + w]);  // j = i-16+w
+    const int L = min(kMaxLevel, M + 1);
+    packed |= (uint32_t)(D | (L << 4)) << (8 * q);
+#pragma unroll
+    for (int d = 0; d < kDepths; d++) cnt[d] += (D <= d && d <= L) ? 1u : 0u;
+    cnt[11] += (D <= L) ? 1u : 0u;
+  }
+  // store packed bytes (4 consecutive particles per thread)
+  if (base + tid * kFlagPer < N) {
+    if (base + tid * kFlagPer + kFlagPer <= N) {
+      reinterpret_cast<uint32_t*>(b.dl)[(base >> 2) + tid] = packed;
+    } else {
+      for (int q = 0; q < kFlagPer && base + tid * kFlagPer + q < N; q++)
+        b.dl[base + tid * kFlagPer + q] = (uint8_t)(packed >> (8 * q));
+    }
+  }
+  const int warp = tid >> 5, lane = tid & 31;
+#pragma unroll
+  for (int k = 0; k < kCounters; k++) {
+    const uint32_t v = __reduce_add_sync(0xffffffffu, cnt[k]);
+    if (lane == 0) s_red[warp][k] = v;
+  }
+  __syncthreads();
+  if (tid < kCounters) {
+    uint32_t s = 0;
+    for (int w = 0; w < kFlagThreads / 32; w++) s += s_red[w][tid];
+    b.blk_counts[(size_t)blockIdx.x * kCounters + tid] = s;
+  }
+}
+
+// K2: one block scans the per-block counts and fills TreeMeta.
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) tree_scan_kernel(BuildBuffers b, uint32_t nblocks,
+                                                                  double root_size,
+                                                                  const MortonFrame* frame,
+                                                                  DevState* st) {
+  __shared__ uint32_t s_warp[kScanThreads / 32][kCounters];
+  __shared__ uint32_t s_tot[kCounters];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t per = (nblocks + kScanThreads - 1) / kScanThreads;
+  const uint32_t b0 = tid * per, b1 = min(nblocks, b0 + per);
+  uint32_t sum[kCounters];
+#pragma unroll
+  for (int k = 0; k < kCounters; k++) sum[k] = 0;
+  for (uint32_t x = b0; x < b1; x++)
+#pragma unroll
+    for (int k = 0; k < kCounters; k++) sum[k] += b.blk_counts[(size_t)x * kCounters + k];
+  uint32_t excl[kCounters];
+#pragma unroll
+  for (int k = 0; k < kCounters; k++) {
+    uint32_t inc = sum[k];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    excl[k] = inc - sum[k];
+    if (lane == 31) s_warp[warp][k] = inc;
+  }
+  __syncthreads();
+  if (tid < kCounters) {
+    uint32_t run = 0;
+    for (int w = 0; w < kScanThreads / 32; w++) {
+      const uint32_t t = s_warp[w][tid];
+      s_warp[w][tid] = run;
+      run += t;
+    }
+    s_tot[tid] = run;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kCounters; k++) excl[k] += s_warp[warp][k];
+  for (uint32_t x = b0; x < b1; x++)
+#pragma unroll
+    for (int k = 0; k < kCounters; k++) {
+      const uint32_t c = b.blk_counts[(size_t)x * kCounters + k];
+      b.blk_offs[(size_t)x * kCounters + k] = excl[k];
+      excl[k] += c;
+    }
+  if (tid == 0) {
+    TreeMeta m;
+    uint32_t run = 0, levels = 0;
+    for (int d = 0; d < kDepths; d++) {
+      m.level_start[d] = run;
+      m.level_count[d] = s_tot[d];
+      run += s_tot[d];
+      if (s_tot[d]) levels = d + 1;
+    }
+    m.level_start[kDepths] = run;
+    m.level_count[kDepths] = 0;
+    m.num_nodes = run;
+    m.num_levels = levels;
+    m.num_leaves = s_tot[11];
+    m.overflow = run > b.cap ? 1u : 0u;
+    m.root_size = frame ? frame->size : root_size;
+    *b.meta = m;
+    if (m.overflow && st) raise_err(st, GS_DERR_NODES);
+  }
+}
+
+// K3: node indices, parents, child bases, leaf lists.
+__global__ void __launch_bounds__(kFlagThreads) tree_emit_kernel(BuildBuffers b, DevState* st) {
+  __shared__ uint32_t s_warp[kFlagThreads / 32][kCounters];
+  __shared__ TreeMeta s_meta;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int64_t base = (int64_t)blockIdx.x * kFlagTile;
+  const uint32_t N = b.N;
+  if (tid == 0) s_meta = *b.meta;
+  uint8_t dl[kFlagPer];
+  uint32_t cnt[kCounters];
+#pragma unroll
+  for (int k = 0; k < kCounters; k++) cnt[k] = 0;
+#pragma unroll
+  for (int q = 0; q < kFlagPer; q++) {
+    const int64_t i = base + tid * kFlagPer + q;
+    dl[q] = i < N ? b.dl[i] : (uint8_t)0;
+    const int D = dl[q] & 15, L = dl[q] >> 4;
+    if (i < N) {
+#pragma unroll
+      for (int d = 0; d < kDepths; d++) cnt[d] += (D <= d && d <= L) ? 1u : 0u;
+      cnt[11] += (D <= L) ? 1u : 0u;
+    }
+  }
+  uint32_t excl[kCounters];
+#pragma unroll
+  for (int k = 0; k < kCounters; k++) {
+    uint32_t inc = cnt[k];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    excl[k] = inc - cnt[k];
+    if (lane == 31) s_warp[warp][k] = inc;
+  }
+  __syncthreads();
+  if (tid < kCounters) {
+    uint32_t run = b.blk_offs[(size_t)blockIdx.x * kCounters + tid];
+    for (int w = 0; w < kFlagThreads / 32; w++) {
+      const uint32_t t = s_warp[w][tid];
+      s_warp[w][tid] = run;
+      run += t;
+    }
+  }
+  __syncthreads();
+  if (s_meta.overflow) return;
+#pragma unroll
+  for (int k = 0; k < kCounters; k++) excl[k] += s_warp[warp][k];
+  const uint32_t* LS = s_meta.level_start;
+#pragma unroll
+  for (int q = 0; q < kFlagPer; q++) {
+    const int64_t i = base + tid * kFlagPer + q;
+    if (i >= N) break;
+    const int D = dl[q] & 15, L = dl[q] >> 4;
+    for (int d = D; d <= L; d++) {
+      const uint32_t n = LS[d] + excl[d];
+      b.node_start[n] = (uint32_t)i;
+      b.depth[n] = (uint8_t)d;
+      // first depth-(d+1) node at or after particle i (children of n start here)
+      b.child_base[n] = d < kMaxLevel ? LS[d + 1] + excl[d + 1] : LS[kDepths];
+      // parent: the depth-(d-1) node containing i (inclusive count - 1)
+      b.parent[n] = d == 0 ? -1
+                           : (int32_t)(LS[d - 1] + excl[d - 1] +
+                                       ((D <= d - 1 && d - 1 <= L) ? 1u : 0u) - 1u);
+      if (d == L) {
+        b.leaf_node[excl[11]] = n;
+        b.leaf_start[excl[11]] = (uint32_t)i;
+      }
+      // mortonTree.js:127: an internal node with numNodes + 8 > maxNodes would be a leaf
+      if (d < L && n + 1 + 8 > b.max_nodes && st) raise_err(st, GS_DERR_NODES);
+    }
+#pragma unroll
+    for (int d = 0; d < kDepths; d++) excl[d] += (D <= d && d <= L) ? 1u : 0u;
+    excl[11] += (D <= L) ? 1u : 0u;
+  }
+}
+
+__device__ inline uint32_t child_count(const BuildBuffers& b, const TreeMeta& m, uint32_t p) {
+  const int d = b.depth[p];
+  const uint32_t cb = b.child_base[p];
+  const uint32_t level_end = m.level_start[d] + m.level_count[d];
+  const uint32_t next = (p + 1 < level_end) ? __ldcg(&b.child_base[p + 1])
+                                            : m.level_start[d + 1] + m.level_count[d + 1];
+  return next - cb;
+}
+
+// COM precision modes of the leaves-up pass.
+enum ComMode : int {
+  kComF32 = 0,   // refresh_level arithmetic (nbody_bh.wgsl:289-313), FP32
+  kComJs = 1,    // MortonTree.build arithmetic (mortonTree.js:130-137, :166-181), double
+  kComF64 = 2,   // FP32 leaves, FP64 internal nodes (large-node reduction in double)
+};
+
+// K4: one thread per leaf; leaf COM, then carry each finished node to its
+// parent; the last child to finish sums the parent (children in slot order).
+template <int MODE>
+__global__ void __launch_bounds__(256) tree_leaves_kernel(BuildBuffers b, const float4* __restrict__ pos,
+                                                          uint32_t pos_stride, DevState* st) {
+  __shared__ TreeMeta s_meta;
+  if (threadIdx.x == 0) s_meta = *b.meta;
+  __syncthreads();
+  const TreeMeta& m = s_meta;
+  if (m.overflow) return;
+  const uint32_t nleaves = m.num_leaves;
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nleaves; r += gridDim.x * blockDim.x) {
+    uint32_t n = b.leaf_node[r];
+    const uint32_t lo = b.leaf_start[r];
+    const uint32_t hi = (r + 1 < nleaves) ? b.leaf_start[r + 1] : b.N;
+    if (n >= m.num_nodes || hi < lo || hi > b.N) {  // impossible for a correct emit
+      if (st) raise_err(st, GS_DERR_NODES);
+      continue;
+    }
+    const int d = b.depth[n];
+    const float size = __double2float_rn(ldexp(m.root_size, -d));
+    float4 c;
+    if (MODE == kComJs) {
+      double mm = 0, cx = 0, cy = 0, cz = 0;
+      for (uint32_t j = lo; j < hi; j++) {
+        const float4 p = pos[(size_t)j * pos_stride];
+        const double pm = p.w;
+        mm = __dadd_rn(mm, pm);
+        cx = __dadd_rn(cx, __dmul_rn((double)p.x, pm));
+        cy = __dadd_rn(cy, __dmul_rn((double)p.y, pm));
+        cz = __dadd_rn(cz, __dmul_rn((double)p.z, pm));
+      }
+      const double inv = mm > 0 ? __ddiv_rn(1.0, mm) : 0.0;
+      c = make_float4(__double2float_rn(__dmul_rn(cx, inv)), __double2float_rn(__dmul_rn(cy, inv)),
+                      __double2float_rn(__dmul_rn(cz, inv)), __double2float_rn(mm));
+    } else {
+      float mm = 0, cx = 0, cy = 0, cz = 0;
+      for (uint32_t j = lo; j < hi; j++) {
+        const float4 p = pos[(size_t)j * pos_stride];
+        cx = fmaf(p.x, p.w, cx);
+        cy = fmaf(p.y, p.w, cy);
+        cz = fmaf(p.z, p.w, cz);
+        mm += p.w;
+      }
+      c = mm > 0.0f ? make_float4(cx / mm, cy / mm, cz / mm, mm) : make_float4(0.f, 0.f, 0.f, mm);
+    }
+    b.cm[n] = c;
+    WalkInfo w;
+    w.s2 = size * size;
+    w.child = lo;
+    w.info = kLeafBit | (hi - lo);
+    w.size = size;
+    b.info[n] = w;
+    // carry upwards
+    while (true) {
+      const int32_t p = b.parent[n];
+      if (p < 0) break;
+      const uint32_t nc = (uint32_t)p < n ? child_count(b, m, (uint32_t)p) : 0u;
+      if ((uint32_t)p >= n || nc == 0 || nc > 8 ||
+          (uint64_t)b.child_base[p] + nc > m.num_nodes) {  // parents precede children in BFS
+        if (st) raise_err(st, GS_DERR_NODES);
+        break;
+      }
+      __threadfence();
+      const uint32_t old = atomicAdd(&b.arrive[p], 1u);
+      if (old + 1 != nc) break;
+      b.arrive[p] = 0;
+      __threadfence();
+      const uint32_t cb = b.child_base[p];
+      float4 pc;
+      if (MODE == kComF32) {
+        float mm = 0, cx = 0, cy = 0, cz = 0;
+        for (uint32_t k = 0; k < nc; k++) {
+          const float4 q = __ldcg(&b.cm[cb + k]);
+          cx = fmaf(q.x, q.w, cx);
+          cy = fmaf(q.y, q.w, cy);
+          cz = fmaf(q.z, q.w, cz);
+          mm += q.w;
+        }
+        pc = mm > 0.0f ? make_float4(cx / mm, cy / mm, cz / mm, mm) : make_float4(0.f, 0.f, 0.f, mm);
+      } else {
+        double mm = 0, cx = 0, cy = 0, cz = 0;
+        for (uint32_t k = 0; k < nc; k++) {
+          const float4 q = __ldcg(&b.cm[cb + k]);
+          const double qm = q.w;
+          mm = __dadd_rn(mm, qm);
+          cx = __dadd_rn(cx, __dmul_rn((double)q.x, qm));
+          cy = __dadd_rn(cy, __dmul_rn((double)q.y, qm));
+          cz = __dadd_rn(cz, __dmul_rn((double)q.z, qm));
+        }
+        if (MODE == kComJs) {
+          const double inv = mm > 0 ? __ddiv_rn(1.0, mm) : 0.0;
+          pc = make_float4(__double2float_rn(__dmul_rn(cx, inv)),
+                           __double2float_rn(__dmul_rn(cy, inv)),
+                           __double2float_rn(__dmul_rn(cz, inv)), __double2float_rn(mm));
+        } else {
+          pc = mm > 0 ? make_float4(__double2float_rn(cx / mm), __double2float_rn(cy / mm),
+                                    __double2float_rn(cz / mm), __double2float_rn(mm))
+                      : make_float4(0.f, 0.f, 0.f, __double2float_rn(mm));
+        }
+      }
+      const int dp = b.depth[p];
+      const float psize = __double2float_rn(ldexp(m.root_size, -dp));
+      b.cm[p] = pc;
+      WalkInfo pw;
+      pw.s2 = psize * psize;
+      pw.child = cb;
+      pw.info = nc;
+      pw.size = psize;
+      b.info[p] = pw;
+      n = (uint32_t)p;
+    }
+  }
+}
+
+// BHNode materialisation (API only): the 64-byte layout of mortonTree.js:12-20.
+__global__ void tree_bhnode_kernel(BuildBuffers b, gs_node* out) {
+  const TreeMeta m = *b.meta;
+  for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < m.num_nodes; n += gridDim.x * blockDim.x) {
+    const float4 c = b.cm[n];
+    const WalkInfo w = b.info[n];
+    gs_node o;
+    o.com[0] = c.x;
+    o.com[1] = c.y;
+    o.com[2] = c.z;
+    o.mass = c.w;
+    o.size = w.size;
+    for (int k = 0; k < 8; k++) o.children[k] = -1;
+    if (w.info & kLeafBit) {
+      o.isLeaf = 1;
+      o.first = w.child;
+      o.count = w.info & ~kLeafBit;
+    } else {
+      o.isLeaf = 0;
+      o.first = 0;
+      o.count = 0;
+      const int shift = 27 - 3 * min((int)b.depth[n], 9);
+      for (uint32_t k = 0; k < w.info && k < 8; k++) {
+        const uint32_t ch = w.child + k;
+        if (ch >= m.num_nodes) break;
+        const uint32_t ps = b.node_start[ch];
+        if (ps >= b.N) break;
+        const uint32_t oct = (b.codes[ps] >> shift) & 7u;
+        o.children[oct] = (int32_t)ch;
+      }
+    }
+    out[n] = o;
+  }
+}
+
+}  // namespace gs

@@ -1,0 +1,149 @@
+// Stable LSD radix sort of 32-bit keys with a 32-bit payload, one kernel per
+// 8-bit digit ("onesweep": per-tile ranking by warp match, decoupled look-back
+// for the tile's global digit offsets, direct scatter). A stable sort of
+// (code, original index) gives exactly the permutation of radixSortIndices
+// (src/physics/mortonTree.js:68-84): ties keep their original order.
+#pragma once
+#include "common.cuh"
+
+namespace gs {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
+constexpr uint32_t kLbAgg = 1u << 30;
+constexpr uint32_t kLbInc = 2u << 30;
+constexpr uint32_t kLbMask = (1u << 30) - 1;
+
+__device__ inline void st_relaxed(uint32_t* p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ inline uint32_t ld_relaxed(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Digit histograms of all passes at once, warp-aggregated. hist: [passes][256].
+__device__ inline void hist_add_warp(uint32_t* s_hist, uint32_t key, bool valid, int passes) {
+  const unsigned lane = threadIdx.x & 31;
+  for (int p = 0; p < passes; p++) {
+    const uint32_t d = (key >> (8 * p)) & 255u;
+    const unsigned peers = __match_any_sync(0xffffffffu, valid ? d : 0x100u + lane);
+    if (valid && (__ffs(peers) - 1) == (int)lane) atomicAdd(&s_hist[p * 256 + d], __popc(peers));
+  }
+}
+
+// One digit pass. FIRST: payload = source index. keys_out may alias nothing.
+template <bool FIRST>
+__global__ void __launch_bounds__(kSortThreads)
+    onesweep_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+                  uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
+                  const uint32_t* __restrict__ hist, uint32_t* lookback, uint32_t* tile_counter,
+                  uint32_t N, int shift, DevState* st) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_warp[kSortWarps][256];
+  __shared__ uint32_t s_prefix[256];
+  __shared__ uint32_t s_scan[kSortWarps];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
+  for (int i = tid; i < kSortWarps * 256; i += kSortThreads) (&s_warp[0][0])[i] = 0;
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint32_t base = tile * kSortTile + warp * (kSortTile / kSortWarps);
+
+  uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+#pragma unroll
+  for (int k = 0; k < kSortItems; k++) {
+    const uint32_t idx = base + k * 32 + lane;
+    if (idx < N) {
+      key[k] = keys_in[idx];
+      val[k] = FIRST ? idx : vals_in[idx];
+    } else {
+      key[k] = 0xffffffffu;
+      val[k] = 0;
+    }
+  }
+  const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int k = 0; k < kSortItems; k++) {
+    const bool valid = base + k * 32 + lane < N;
+    const uint32_t d = (key[k] >> shift) & 255u;
+    const unsigned peers = __match_any_sync(0xffffffffu, valid ? d : 0x100u + lane);
+    const uint32_t before = valid ? s_warp[warp][d] : 0u;
+    rank[k] = before + __popc(peers & lt);
+    __syncwarp();
+    if (valid && (__ffs(peers) - 1) == lane) s_warp[warp][d] = before + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // Per digit: exclusive scan over warps (stable order warp 0..7) and tile total.
+  const uint32_t d = tid;  // kSortThreads == 256 digits
+  uint32_t tot = 0;
+#pragma unroll
+  for (int w = 0; w < kSortWarps; w++) {
+    const uint32_t c = s_warp[w][d];
+    s_warp[w][d] = tot;
+    tot += c;
+  }
+  // Global exclusive offset of digit d (block-wide exclusive scan of hist).
+  const uint32_t h = hist[d];
+  uint32_t incl = h;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) s_scan[warp] = incl;
+  __syncthreads();
+  uint32_t wpre = 0;
+  for (int w = 0; w < warp; w++) wpre += s_scan[w];
+  const uint32_t gexcl = wpre + incl - h;
+
+  uint32_t* lb = lookback + (size_t)tile * 256;
+  uint32_t excl;
+  if (tile == 0) {
+    excl = gexcl;
+    st_relaxed(&lb[d], kLbInc | (gexcl + tot));
+  } else {
+    st_relaxed(&lb[d], kLbAgg | tot);
+    excl = 0;
+    int64_t t = (int64_t)tile - 1;
+    uint32_t spins = 0;
+    while (t >= 0) {
+      const uint32_t v = ld_relaxed(lookback + (size_t)t * 256 + d);
+      const uint32_t flag = v & ~kLbMask;
+      if (flag == 0) {
+        if (++spins > kSpinLimit) {
+          raise_err(st, GS_DERR_LOOKBACK);
+          break;
+        }
+        continue;
+      }
+      excl += v & kLbMask;
+      if (flag == kLbInc) break;
+      t--;
+    }
+    st_relaxed(&lb[d], kLbInc | ((excl + tot) & kLbMask));
+  }
+  s_prefix[d] = excl;
+  __syncthreads();
+
+#pragma unroll
+  for (int k = 0; k < kSortItems; k++) {
+    if (base + k * 32 + lane < N) {
+      const uint32_t dd = (key[k] >> shift) & 255u;
+      const uint32_t pos = s_prefix[dd] + s_warp[warp][dd] + rank[k];
+      if (pos >= N) {  // only after a failed look-back: flag, never write out of bounds
+        raise_err(st, GS_DERR_LOOKBACK);
+        continue;
+      }
+      keys_out[pos] = key[k];
+      vals_out[pos] = val[k];
+    }
+  }
+}
+
+}  // namespace gs

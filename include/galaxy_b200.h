@@ -1,0 +1,193 @@
+/*
+ * galaxy_b200 — C ABI of the B200 (sm_100a) gravity path of galaxy-sim.
+ *
+ * This is the drop-in boundary for the reference's compute surface:
+ *   - the NBodyGPU class, src/physics/NBodyGPU.js:14-369 (one gs_ctx per
+ *     NBodyGPU instance; the WebGPU command encoder maps to the context's
+ *     CUDA stream order), and
+ *   - the exports of src/physics/mortonTree.js (computeMortonCodes,
+ *     radixSortIndices, MortonTree.build, sortAndBuild) and the rebuild of
+ *     src/physics/bhWorker.js, which run on the GPU here instead of a Web Worker.
+ *
+ * Conventions
+ *   - Every entry point returns an int status (GS_OK = 0, negative on error)
+ *     and never aborts; gs_last_error() describes the last failure of a context
+ *     (gs_last_error(NULL) the last context-free failure of the calling thread).
+ *   - Host pointers are borrowed for the duration of the call only.
+ *   - A context owns all of its device memory; one context = one CUDA stream =
+ *     one host thread at a time.
+ *   - Particle records keep the reference's 32-byte layout
+ *     [x, y, z, m, vx, vy, vz, pad] (nbody_bh.wgsl:10-17) and the 16-byte
+ *     stellar layout [stellarMass, birthMyr, seed, dust] (NBodyGPU.js:83-90);
+ *     tree nodes the 64-byte BHNode layout (nbody_bh.wgsl:47-54 ==
+ *     mortonTree.js:12-20); params the 96-byte Params uniform
+ *     (nbody_bh.wgsl:19-42, NBodyGPU.js:253-275).
+ *   - The particle buffers ping-pong: step and applyPermutation flip them,
+ *     exactly as NBodyGPU.js:236-237, :328 do.
+ */
+#ifndef GALAXY_B200_H
+#define GALAXY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GS_OK 0
+#define GS_EINVAL (-1)     /* bad argument (N, pointer, size, layout) */
+#define GS_ENOMEM (-2)     /* device or pinned-host allocation failed */
+#define GS_ECUDA (-3)      /* a CUDA runtime call failed */
+#define GS_ETIMEDOUT (-4)  /* a bounded host wait expired */
+#define GS_EDEVICE (-5)    /* a kernel raised its error word (see gs_last_error) */
+#define GS_ENOTREADY (-6)  /* the operation needs state that is not there yet */
+
+/* device error-word bits (gs_device_errors) */
+#define GS_DERR_LOOKBACK 0x1u   /* sort look-back wait exceeded its iteration limit */
+#define GS_DERR_STACK 0x2u      /* walk stack deeper than the tree can be */
+#define GS_DERR_NODES 0x4u      /* node pool exhausted */
+#define GS_DERR_TREE 0x8u       /* uploaded tree is not a BFS tree with contiguous children */
+
+typedef struct gs_ctx gs_ctx;
+
+/* 96-byte Params uniform (nbody_bh.wgsl:19-42). */
+typedef struct gs_params {
+  float dt, G, epsilon2;
+  uint32_t N;
+  float theta, haloMass, haloA, gasDrag, time, agingRate, sfDensity, sfEff, sfDt;
+  uint32_t haloCount;
+  float pad0, pad1;
+  float haloC1[4];
+  float haloC2[4];
+} gs_params;
+
+/* 64-byte BHNode (nbody_bh.wgsl:47-54). */
+typedef struct gs_node {
+  float com[3];
+  float mass;
+  float size;
+  uint32_t isLeaf;
+  uint32_t first;
+  uint32_t count;
+  int32_t children[8];
+} gs_node;
+
+/* Energy and momentum diagnostics (nbody_bh.wgsl:180, bhWorker.js:74). */
+typedef struct gs_diag {
+  double e_diag;      /* sum of the specific energies e_i the step wrote (the HUD's E) */
+  double e_true;      /* sum of m_i (1/2 v_i^2 + 1/2 phi_pair_i + phi_halo_i) */
+  double momentum[3]; /* sum of m_i v_i */
+  double mass;        /* sum of m_i */
+} gs_diag;
+
+const char* gs_last_error(const gs_ctx* ctx);
+const char* gs_version(void);
+/* Number of CUDA devices visible; returns GS_OK and writes the count. */
+int gs_device_count(int* count);
+
+/* ---- NBodyGPU surface (NBodyGPU.js) ---------------------------------------------- */
+
+/* NBodyGPU constructor + _init (NBodyGPU.js:15-203): both ping-pong buffers get
+ * the initial particles, both stellar buffers the stellar records. */
+int gs_create(uint32_t N, const float* particles8, const float* stellar4, gs_ctx** out);
+/* Same on an explicit CUDA device ordinal. */
+int gs_create_on(int device, uint32_t N, const float* particles8, const float* stellar4,
+                 gs_ctx** out);
+/* NBodyGPU.destroy (NBodyGPU.js:358-368). */
+int gs_destroy(gs_ctx* ctx);
+/* NBodyGPU.updateParams (NBodyGPU.js:253-275); N is forced to the context's N. */
+int gs_update_params(gs_ctx* ctx, const gs_params* params);
+/* Simulation clock (main.js simTime, a double): full steps stamp
+ * Params.time = f32(simTime) and advance it by dt. gs_update_params sets it to
+ * Params.time; this sets it exactly. */
+int gs_set_time(gs_ctx* ctx, double t);
+/* COM arithmetic of the on-device build's refresh: 0 = FP32 like refresh_level
+ * (nbody_bh.wgsl:289-313), 2 = FP32 leaves with FP64 internal-node sums. */
+int gs_set_com_mode(gs_ctx* ctx, int mode);
+/* NBodyGPU.updateCentralMass (NBodyGPU.js:245-251): both ping-pong buffers. */
+int gs_update_central_mass(gs_ctx* ctx, float mass, uint32_t idx);
+/* NBodyGPU.applyPermutation (NBodyGPU.js:225-238): gather out[i] = in[perm[i]] of
+ * particles and stellar records, then flip both ping-pongs. perm is a host array. */
+int gs_apply_permutation(gs_ctx* ctx, const uint32_t* perm);
+/* NBodyGPU.uploadBHTree (NBodyGPU.js:288-301): level_ranges holds n_levels
+ * [start, count] pairs (at most 16, like the reference's refresh uniform). */
+int gs_upload_tree(gs_ctx* ctx, const gs_node* nodes, uint32_t num_nodes,
+                   const uint32_t* level_ranges, uint32_t n_levels);
+/* NBodyGPU.encodeRefresh (NBodyGPU.js:308-319) → refresh_level deepest first. */
+int gs_refresh(gs_ctx* ctx);
+/* NBodyGPU.step (NBodyGPU.js:321-329): walk + halo + kick-drift, flip. */
+int gs_step(gs_ctx* ctx);
+/* NBodyGPU.encodeStarFormation (NBodyGPU.js:278-285). */
+int gs_star_formation(gs_ctx* ctx);
+/* encodePositionReadback + readPositions (NBodyGPU.js:335-350): vec4(pos, e_i)
+ * per particle into out4 (N*4 floats); waits at most timeout_ns (0 = no limit). */
+int gs_read_positions(gs_ctx* ctx, float* out4, uint64_t timeout_ns);
+/* positionBuffer / stellarBuffer getters (NBodyGPU.js:241-243, :353-356):
+ * device pointers of the current buffers (valid until the next flip). */
+int gs_position_buffer(gs_ctx* ctx, void** dptr);
+int gs_stellar_buffer(gs_ctx* ctx, void** dptr);
+
+/* ---- on-device rebuild (replaces the bhWorker.js round trip) ------------------------ */
+
+/* Track up to two central particles (main.js:272-283) whose smoothed positions
+ * centre the halos: c1/c2 are particle indices (-1 = none), halo_c* the
+ * initial centres (NULL = the particle's current position). */
+int gs_set_tracking(gs_ctx* ctx, int64_t c1, int64_t c2, const double* halo_c1,
+                    const double* halo_c2);
+int gs_get_tracking(gs_ctx* ctx, int64_t* c1, int64_t* c2, double* halo_c1, double* halo_c2);
+/* Morton codes + stable sort + gather (particles, stellar, tracked indices) +
+ * halo-centre EMA (main.js:449-457) + BFS bucketed octree + COM refresh, all on
+ * the device: one bhWorker.js rebuild plus its application in main.js. */
+int gs_sort_build(gs_ctx* ctx);
+/* Full steps: nsteps x [gs_sort_build, walk + halo + kick-drift (+ star
+ * formation when do_sf)], advancing Params.time by dt each step; replayed from a
+ * CUDA graph. */
+int gs_run(gs_ctx* ctx, uint32_t nsteps, int do_sf);
+/* The context's CUDA stream (cudaStream_t), e.g. to record timing events in
+ * its order. */
+int gs_stream(gs_ctx* ctx, void** stream);
+/* Block until the context's stream is idle (bounded by timeout_ns, 0 = none). */
+int gs_sync(gs_ctx* ctx, uint64_t timeout_ns);
+/* Read the current tree in BHNode layout (+ level ranges, permutation of the last
+ * gs_sort_build). Any output pointer may be NULL. */
+int gs_get_tree(gs_ctx* ctx, gs_node* nodes, uint32_t nodes_cap, uint32_t* num_nodes,
+                uint32_t* level_ranges, uint32_t lr_cap, uint32_t* n_levels, uint32_t* perm);
+/* Raw state read/write (checkpoint): N*8 particle floats, N*4 stellar floats. */
+int gs_read_state(gs_ctx* ctx, float* particles8, float* stellar4);
+int gs_write_state(gs_ctx* ctx, const float* particles8, const float* stellar4);
+/* Per-particle pair acceleration + potential {ax, ay, az, phi} (G applied, halo
+ * excluded) and leaf density of the last walk; needs gs_set_debug(ctx, 1) first. */
+int gs_set_debug(gs_ctx* ctx, int enable);
+int gs_read_forces(gs_ctx* ctx, float* acc4, float* density);
+/* FP64 diagnostics of the state the last step wrote. */
+int gs_energy(gs_ctx* ctx, gs_diag* out);
+/* Device error word (GS_DERR_* bits); clear=1 resets it. */
+int gs_device_errors(gs_ctx* ctx, uint32_t* bits, int clear);
+/* Interaction counters of the last walk(s): monopoles, leaf pairs, node visits. */
+int gs_counters(gs_ctx* ctx, uint64_t out[3], int reset);
+
+/* ---- mortonTree.js exports, stateless (host arrays in and out) ---------------------- */
+
+/* computeMortonCodes (mortonTree.js:43-62): returns rootSize through root_size. */
+int gs_morton_codes(const float* pos, uint32_t N, uint32_t stride, uint32_t* codes,
+                    double* root_size);
+/* radixSortIndices (mortonTree.js:68-84): stable sort -> gather permutation. */
+int gs_radix_sort_indices(const uint32_t* codes, uint32_t N, uint32_t* perm);
+/* MortonTree.build (mortonTree.js:107-182) over sorted codes, stride-3 positions
+ * and masses; max_nodes follows the MortonTree pool (2N + 4096 there). */
+int gs_tree_build(const uint32_t* sorted_codes, const float* pos3, const float* masses,
+                  uint32_t N, double root_size, uint32_t max_nodes, gs_node* nodes,
+                  uint32_t* num_nodes, uint32_t* level_ranges, uint32_t lr_cap,
+                  uint32_t* n_levels);
+/* sortAndBuild (mortonTree.js:192-224). */
+int gs_sort_and_build(const float* particles8, const float* stellar4, uint32_t N,
+                      int64_t track_idx2, float* sorted8, float* sorted_stellar4,
+                      uint32_t* perm, gs_node* nodes, uint32_t max_nodes, uint32_t* num_nodes,
+                      uint32_t* level_ranges, uint32_t lr_cap, uint32_t* n_levels,
+                      int64_t* central_idx, int64_t* central_idx2, float* sorted_mass);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GALAXY_B200_H */
