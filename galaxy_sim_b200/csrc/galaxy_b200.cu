@@ -27,7 +27,7 @@ namespace {
 
 thread_local char g_err[512] = "";
 
-constexpr uint32_t kMaxN = 1u << 28;
+constexpr uint32_t kMaxN = 1u << 27;  // node indices (2N + 4096) fit the walk's 29-bit fields
 constexpr int kSortPasses = 4;
 
 inline uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
@@ -225,7 +225,9 @@ struct gs_ctx {
   gs_params hp{};
   double* partials = nullptr;
   double* diag_out = nullptr;
-  uint32_t walk_blocks = 0;
+  uint32_t walk_groups = 0;  // 32-particle groups (diagnostic partials)
+  uint32_t walk_grid = 0;    // persistent walk blocks
+  unsigned* walk_work = nullptr;
   float4* dbg_acc = nullptr;
   float* dbg_dens = nullptr;
   bool debug = false;
@@ -323,12 +325,14 @@ void enqueue_walk(gs_ctx* c, int sf) {
   a.partials = c->partials;
   a.N = c->N;
   a.node_cap = c->ws.cap;
+  a.work = c->walk_work;
+  const uint32_t g = c->walk_grid;
   if (c->debug) {
-    if (sf) walk_kernel<true, true><<<c->walk_blocks, kWalkThreads, 0, c->stream>>>(a);
-    else walk_kernel<false, true><<<c->walk_blocks, kWalkThreads, 0, c->stream>>>(a);
+    if (sf) walk_kernel<true, true><<<g, kWalkThreads, 0, c->stream>>>(a);
+    else walk_kernel<false, true><<<g, kWalkThreads, 0, c->stream>>>(a);
   } else {
-    if (sf) walk_kernel<true, false><<<c->walk_blocks, kWalkThreads, 0, c->stream>>>(a);
-    else walk_kernel<false, false><<<c->walk_blocks, kWalkThreads, 0, c->stream>>>(a);
+    if (sf) walk_kernel<true, false><<<g, kWalkThreads, 0, c->stream>>>(a);
+    else walk_kernel<false, false><<<g, kWalkThreads, 0, c->stream>>>(a);
   }
   c->cur ^= 1;
 }
@@ -463,9 +467,17 @@ int gs_create_on(int device, uint32_t N, const float* particles8, const float* s
   if ((rc = c->cuda(w.alloc(&c->compact, N), "compact"))) return bail(rc);
   if ((rc = c->cuda(w.alloc(&c->perm_user, N), "perm"))) return bail(rc);
   if ((rc = c->cuda(w.alloc(&c->st, 1), "state"))) return bail(rc);
-  c->walk_blocks = cdiv(N, kWalkThreads);
-  if ((rc = c->cuda(w.alloc(&c->partials, (size_t)c->walk_blocks * kPartials), "partials")))
+  c->walk_groups = cdiv(N, 32);
+  {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    c->walk_grid = std::min<uint32_t>(cdiv(c->walk_groups, kWalkWarps),
+                                      (uint32_t)sms * kWalkBlocksPerSM);
+  }
+  if ((rc = c->cuda(w.alloc(&c->partials, (size_t)c->walk_groups * kPartials), "partials")))
     return bail(rc);
+  if ((rc = c->cuda(w.alloc(&c->walk_work, 4), "walk counters"))) return bail(rc);
+  if ((rc = c->cuda(cudaMemset(c->walk_work, 0, 16), "walk counters"))) return bail(rc);
   if ((rc = c->cuda(w.alloc(&c->diag_out, 8), "diag"))) return bail(rc);
   if ((rc = c->cuda(cudaMallocHost(&c->host_stage, (size_t)N * 16 + 256), "pinned stage")))
     return bail(rc);
@@ -489,7 +501,7 @@ int gs_create_on(int device, uint32_t N, const float* particles8, const float* s
   c->hp = st0.p;
   if ((rc = c->cuda(cudaMemcpy(c->st, &st0, sizeof(st0), cudaMemcpyHostToDevice), "state")))
     return bail(rc);
-  if ((rc = c->cuda(cudaMemset(c->partials, 0, sizeof(double) * c->walk_blocks * kPartials), "m")))
+  if ((rc = c->cuda(cudaMemset(c->partials, 0, sizeof(double) * c->walk_groups * kPartials), "m")))
     return bail(rc);
   *out = c;
   return GS_OK;
@@ -844,7 +856,7 @@ int gs_read_forces(gs_ctx* ctx, float* acc4, float* density) {
 int gs_energy(gs_ctx* ctx, gs_diag* out) {
   CTX_CHECK(ctx);
   if (!out) return ctx->fail(GS_EINVAL, "out is NULL");
-  diag_reduce_kernel<<<1, dim3(32, kPartials), 0, ctx->stream>>>(ctx->partials, ctx->walk_blocks,
+  diag_reduce_kernel<<<1, dim3(32, kPartials), 0, ctx->stream>>>(ctx->partials, ctx->walk_groups,
                                                                   ctx->diag_out);
   CK(ctx, cudaGetLastError(), "diag");
   double h[kPartials];

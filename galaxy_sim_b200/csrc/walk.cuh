@@ -7,12 +7,20 @@
 // v += a dt, gas drag, x += v dt, pad and specific-energy writes.
 //
 // Execution is warp-cooperative: a warp owns 32 Morton-consecutive particles
-// (one per lane) and walks the union of their frontiers with a warp-uniform
-// stack of child ranges (children of a BFS node are contiguous), so every node
-// and leaf particle is a broadcast load. Each lane still applies exactly its
-// own particle's acceptance decisions: a lane is active for a node only if it
-// opened every ancestor, so the per-particle interaction set is identical to
+// (one per lane) and walks the union of their frontiers, but each lane applies
+// exactly its own particle's acceptance decisions (a lane is active for a node
+// only if it opened every ancestor), so the per-particle interaction set equals
 // the reference's thread-per-particle stack walk.
+//   * The stack holds child ranges (children of a BFS node are contiguous) with
+//     the mask of lanes that opened the parent; a popped range is staged into
+//     shared memory by one coalesced load (one child per lane) in
+//     structure-of-arrays form.
+//   * Children are tested two at a time, and an opened leaf's particles are
+//     staged the same way and summed two at a time, with sm_100's packed
+//     FP32x2 FMA/ADD/MUL; accumulation is predicated, not branched.
+//   * Warps are persistent and take 32-particle groups from an atomic counter
+//     (load balance across the dense core); per-group FP64 partials of the
+//     diagnostics replace a block-wide barrier.
 #pragma once
 #include "common.cuh"
 
@@ -21,6 +29,8 @@ namespace gs {
 constexpr int kWalkThreads = 128;
 constexpr int kWalkWarps = kWalkThreads / 32;
 constexpr int kPartials = 6;  // e_diag, e_true, px, py, pz, mass
+constexpr int kWalkStack = 96;  // ranges; a range push per opened node, <= 7 * depth + 1
+constexpr int kWalkBlocksPerSM = 8;
 
 // nbody_bh.wgsl:206-213
 __device__ inline uint32_t pcg(uint32_t v0) {
@@ -48,7 +58,7 @@ __device__ inline uint32_t wgsl_u32(float x) {
 }
 
 // star_formation (nbody_bh.wgsl:229-268) on one particle, in registers.
-// p0 = (pos, mass), p1 = (vel, pad), s = stellar record. Returns true if changed.
+// p1 = (vel, pad), s = stellar record.
 __device__ inline void star_formation_one(const gs_params& P, uint32_t i, float4& p1, float4& s) {
   const uint32_t salt = wgsl_u32(__fmul_rn(P.time, 977.0f)) + 1u;
   if (p1.w < -0.5f) {
@@ -86,209 +96,321 @@ struct WalkArgs {
   float* __restrict__ energy;       // e_i
   float4* __restrict__ dbg_acc;     // optional {ax, ay, az, phi} (G applied)
   float* __restrict__ dbg_dens;
-  double* __restrict__ partials;    // [blocks][kPartials]
+  double* __restrict__ partials;    // [groups][kPartials]
+  unsigned* work;                   // [0] next group, [1] finished warps (self-resetting)
   uint32_t N;
   uint32_t node_cap;                // allocated nodes: child ranges must stay below it
 };
 
+// Per-warp shared staging.
+struct WalkSmem {
+  uint2 stack[kWalkStack];          // {first child | (count-1) << 29, lane mask}
+  float cx[10], cy[10], cz[10], cmass[10], cs2[10];
+  uint4 cmeta[10];                  // {child, info, own-leaf density bits, 0}
+  float lx[34], ly[34], lz[34], lm[34];
+};
+
+__device__ inline float2 f2(float a) { return make_float2(a, a); }
+
+__device__ inline void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 template <bool SF, bool DBG>
-__global__ void __launch_bounds__(kWalkThreads) walk_kernel(WalkArgs a) {
-  __shared__ double s_part[kWalkWarps][kPartials];
+__global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(WalkArgs a) {
+  __shared__ WalkSmem smem_all[kWalkWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t i = blockIdx.x * kWalkThreads + threadIdx.x;
-  const bool valid = i < a.N;
-  const gs_params P = a.st->p;
-  const float eps2 = P.epsilon2;
-  const float theta2 = P.theta * P.theta;
+  WalkSmem& S = smem_all[warp];
+  const gs_params& P = a.st->p;  // read-only during the walk; fields loaded where used
+  const float eps2 = __ldg(&P.epsilon2);
+  const float theta2 = __ldg(&P.theta) * __ldg(&P.theta);
   const float qe2 = 0.25f * eps2;
+  const bool soft = eps2 > 0.0f;  // self pairs may then be summed and removed afterwards
+  const uint32_t ngroups = (a.N + 31) / 32;
+  const unsigned full = 0xffffffffu;
 
-  float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0;
-  if (valid) {
-    p0 = a.pin[2 * (size_t)i];
-    p1 = a.pin[2 * (size_t)i + 1];
-  }
-  float ax = 0.f, ay = 0.f, az = 0.f, pot = 0.f, dens = 0.f;
-  unsigned long long nmono = 0, npair = 0, nvisit = 0;
-  const unsigned all = __ballot_sync(0xffffffffu, valid);
-
-  // warp-uniform stack of child ranges; lane k holds entry k
-  uint32_t s_start = 0, s_cnt = 0, s_mask = 0;
-  int sp = 0;
-  if (all) {
-    if (lane == 0) {
-      s_start = 0;
-      s_cnt = 1;
-      s_mask = all;
+  while (true) {
+    uint32_t g = 0;
+    if (lane == 0) g = atomicAdd(&a.work[0], 1u);
+    g = __shfl_sync(full, g, 0);
+    if (g >= ngroups) break;
+    const uint32_t gbeg = g * 32, gend = gbeg + 32;
+    const uint32_t i = gbeg + lane;
+    const bool valid = i < a.N;
+    float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0;
+    if (valid) {
+      p0 = a.pin[2 * (size_t)i];
+      p1 = a.pin[2 * (size_t)i + 1];
     }
+    const float2 px = f2(-p0.x), py = f2(-p0.y), pz = f2(-p0.z);  // negated: r = q + (-p)
+    float2 ax = f2(0.f), ay = f2(0.f), az = f2(0.f), pt = f2(0.f);
+    float dens = 0.f, selfw = 0.f;
+    unsigned long long nmono = 0, npair = 0, nvisit = 0;
+    const unsigned all = __ballot_sync(full, valid);
+
+    int sp = 0;
+    if (lane == 0) S.stack[0] = make_uint2(0u, all);  // the root: range {0, 1}
     sp = 1;
-  }
-  // A well-formed tree is visited at most once per node; the cap only bounds the
-  // loop if the node data were ever corrupted.
-  uint32_t budget = 4u * a.node_cap + 1024u;
-  while (sp > 0) {
-    if (--budget == 0) {
-      if (lane == 0) raise_err(a.st, GS_DERR_STACK);
-      break;
-    }
-    const int top = sp - 1;
-    const uint32_t n = __shfl_sync(0xffffffffu, s_start, top);
-    const uint32_t c = __shfl_sync(0xffffffffu, s_cnt, top);
-    const uint32_t mask = __shfl_sync(0xffffffffu, s_mask, top);
-    if (lane == top) {
-      s_start++;
-      s_cnt--;
-    }
-    if (c == 1) sp--;
-    const float4 q = __ldg(&a.cm[n]);
-    if (q.w == 0.0f) continue;
-    const WalkInfo w = a.info[n];
-    const bool act = (mask >> lane) & 1u;
-    const bool leaf = (w.info & kLeafBit) != 0u;
-    const uint32_t cnt = w.info & ~kLeafBit;
-    if (DBG) nvisit += act;
-    if (leaf && act && (i - w.child) < cnt) dens = (float)cnt / (w.size * w.size * w.size);
-    const float rx = q.x - p0.x, ry = q.y - p0.y, rz = q.z - p0.z;
-    const float d2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps2)));
-    const bool ok = (w.s2 < theta2 * d2) || (w.s2 < qe2);
-    if (act && ok) {
-      const float rinv = rsqrtf(d2);
-      const float mr = q.w * rinv;
-      const float f = mr * rinv * rinv;
-      ax = fmaf(rx, f, ax);
-      ay = fmaf(ry, f, ay);
-      az = fmaf(rz, f, az);
-      pot -= mr;
-      if (DBG) nmono++;
-    }
-    const unsigned open = __ballot_sync(0xffffffffu, act && !ok);
-    if (open) {
-      // children come after their parent and stay inside the node / particle arrays
-      const bool sane = leaf ? ((uint64_t)w.child + cnt <= a.N)
-                             : (w.child > n && (uint64_t)w.child + cnt <= a.node_cap && cnt <= 8u);
-      if (!sane) {
-        if (lane == 0) raise_err(a.st, GS_DERR_TREE);
-        continue;
+    uint32_t budget = 4u * a.node_cap + 1024u;
+    while (sp > 0) {
+      __syncwarp();
+      const uint2 e = S.stack[--sp];
+      const uint32_t start = e.x & 0x1fffffffu;
+      const uint32_t cnt = (e.x >> 29) + 1u;
+      const unsigned mask = e.y;
+      if (--budget == 0) {
+        if (lane == 0) raise_err(a.st, GS_DERR_STACK);
+        break;
       }
-      if (leaf) {
-        const bool me = (open >> lane) & 1u;
-        const uint32_t end = w.child + cnt;
-        for (uint32_t j = w.child; j < end; j++) {
-          const float4 pj = __ldg(&a.pin[2 * (size_t)j]);
-          if (me) {
-            const float jx = pj.x - p0.x, jy = pj.y - p0.y, jz = pj.z - p0.z;
-            const float e2 = fmaf(jx, jx, fmaf(jy, jy, fmaf(jz, jz, eps2)));
-            const float rinv = rsqrtf(e2);
-            const float mj = (j == i) ? 0.0f : pj.w;
-            const float mr = mj * rinv;
-            const float f = mr * rinv * rinv;
-            ax = fmaf(jx, f, ax);
-            ay = fmaf(jy, f, ay);
-            az = fmaf(jz, f, az);
-            pot -= mr;
-            if (DBG) npair += (j != i);
+      __syncwarp();
+      // stage the range: one child per lane, plus a massless partner for an odd count
+      bool own = false;
+      if (lane <= (int)cnt) {
+        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+        WalkInfo w;
+        w.s2 = 0.f;
+        w.child = 0;
+        w.info = kLeafBit;
+        w.size = 1.f;
+        if (lane < (int)cnt) {
+          q = __ldg(&a.cm[start + lane]);
+          w = a.info[start + lane];
+        }
+        const uint32_t wc = w.info & ~kLeafBit;
+        own = (w.info & kLeafBit) && q.w != 0.0f && w.child < gend && w.child + wc > gbeg;
+        S.cx[lane] = q.x;
+        S.cy[lane] = q.y;
+        S.cz[lane] = q.z;
+        S.cmass[lane] = q.w;
+        S.cs2[lane] = w.s2;
+        S.cmeta[lane] = make_uint4(w.child, w.info,
+                                   own ? __float_as_uint((float)wc / (w.size * w.size * w.size)) : 0u, 0u);
+      }
+      const unsigned ownmask = __ballot_sync(full, own);  // leaves holding this warp's particles
+      __syncwarp();
+      const bool act = (mask >> lane) & 1u;
+      for (uint32_t c = 0; c < cnt; c += 2) {
+        const float2 qx = *reinterpret_cast<const float2*>(&S.cx[c]);
+        const float2 qy = *reinterpret_cast<const float2*>(&S.cy[c]);
+        const float2 qz = *reinterpret_cast<const float2*>(&S.cz[c]);
+        const float2 qm = *reinterpret_cast<const float2*>(&S.cmass[c]);
+        const float2 s2 = *reinterpret_cast<const float2*>(&S.cs2[c]);
+        const float2 rx = __fadd2_rn(qx, px), ry = __fadd2_rn(qy, py), rz = __fadd2_rn(qz, pz);
+        const float2 d2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __ffma2_rn(rz, rz, f2(eps2))));
+        const float2 td = __fmul2_rn(f2(theta2), d2);
+        const bool live0 = act && qm.x != 0.0f, live1 = act && qm.y != 0.0f;
+        const bool ok0 = (s2.x < td.x) || (s2.x < qe2);
+        const bool ok1 = (s2.y < td.y) || (s2.y < qe2);
+        const bool acc0 = live0 && ok0, acc1 = live1 && ok1;
+        const float2 rinv = make_float2(acc0 ? rsqrtf(d2.x) : 0.0f, acc1 ? rsqrtf(d2.y) : 0.0f);
+        const float2 mr = __fmul2_rn(qm, rinv);
+        const float2 f = __fmul2_rn(__fmul2_rn(mr, rinv), rinv);
+        ax = __ffma2_rn(rx, f, ax);
+        ay = __ffma2_rn(ry, f, ay);
+        az = __ffma2_rn(rz, f, az);
+        pt = __fadd2_rn(pt, mr);  // sum of m/r; potential = -G * sum
+        if (DBG) {
+          nmono += acc0 + acc1;
+          nvisit += live0 + live1;
+        }
+        // own-leaf density (nbody_bh.wgsl:93-95): only leaves that hold this warp's particles
+        if ((ownmask >> c) & 3u) {
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            if (!((ownmask >> (c + h)) & 1u)) continue;
+            const uint4 mt = S.cmeta[c + h];
+            if ((h ? live1 : live0) && (i - mt.x) < (mt.y & ~kLeafBit)) dens = __uint_as_float(mt.z);
           }
         }
-      } else {
-        if (sp >= 31) {  // cannot happen for depth <= 10 trees; never corrupt the stack
-          if (lane == 0) raise_err(a.st, GS_DERR_STACK);
-          break;
+        const bool op0 = live0 && !ok0, op1 = live1 && !ok1;
+        if (!__ballot_sync(full, op0 || op1)) continue;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const uint32_t cc = c + h;
+          const unsigned open = __ballot_sync(full, h ? op1 : op0);
+          if (!open) continue;
+          const uint4 mt = S.cmeta[cc];
+          const uint32_t cchild = mt.x;
+          const bool leaf = (mt.y & kLeafBit) != 0u;
+          const uint32_t ccnt = mt.y & ~kLeafBit;
+          const bool sane = leaf ? ((uint64_t)cchild + ccnt <= a.N)
+                                 : (cchild > start + cc && (uint64_t)cchild + ccnt <= a.node_cap &&
+                                    ccnt >= 1u && ccnt <= 8u);
+          if (!sane) {
+            if (lane == 0) raise_err(a.st, GS_DERR_TREE);
+            continue;
+          }
+          if (!leaf) {
+            if (sp >= kWalkStack) {  // cannot happen for depth <= 10 trees
+              if (lane == 0) raise_err(a.st, GS_DERR_STACK);
+              continue;
+            }
+            if (lane == 0) S.stack[sp] = make_uint2(cchild | ((ccnt - 1u) << 29), open);
+            if (lane < (int)ccnt) {  // warm L1 for the range's staging load
+              prefetch_l1(&a.cm[cchild + lane]);
+              prefetch_l1(&a.info[cchild + lane]);
+            }
+            sp++;
+            continue;
+          }
+          // leaf direct sum over [cchild, cchild + ccnt), two sources at a time
+          const bool me = (open >> lane) & 1u;
+          const float2 wme = f2(me ? 1.0f : 0.0f);
+          for (uint32_t b0 = 0; b0 < ccnt; b0 += 32) {
+            const uint32_t k = min(32u, ccnt - b0);
+            __syncwarp();
+            if (lane < (int)k) {
+              const float4 q = __ldg(&a.pin[2 * (size_t)(cchild + b0 + lane)]);
+              S.lx[lane] = q.x;
+              S.ly[lane] = q.y;
+              S.lz[lane] = q.z;
+              S.lm[lane] = q.w;
+            } else if (lane == (int)k) {
+              S.lx[lane] = S.ly[lane] = S.lz[lane] = 0.f;
+              S.lm[lane] = 0.f;
+            }
+            __syncwarp();
+            const uint32_t jself = i - (cchild + b0);  // my own slot, if in this chunk
+            if (soft) {
+              // every pair incl. j == i (zero force at r = 0); the self potential
+              // m_i / eps is removed once at the end
+              if (me && jself < k) selfw += 1.0f;
+              for (uint32_t j = 0; j < k; j += 2) {
+                const float2 jx = *reinterpret_cast<const float2*>(&S.lx[j]);
+                const float2 jy = *reinterpret_cast<const float2*>(&S.ly[j]);
+                const float2 jz = *reinterpret_cast<const float2*>(&S.lz[j]);
+                const float2 jm = *reinterpret_cast<const float2*>(&S.lm[j]);
+                const float2 ex = __fadd2_rn(jx, px), ey = __fadd2_rn(jy, py), ez = __fadd2_rn(jz, pz);
+                const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __ffma2_rn(ez, ez, f2(eps2))));
+                const float2 ri = __fmul2_rn(make_float2(rsqrtf(e2.x), rsqrtf(e2.y)), wme);
+                const float2 mr = __fmul2_rn(jm, ri);
+                const float2 ff = __fmul2_rn(__fmul2_rn(mr, ri), ri);
+                ax = __ffma2_rn(ex, ff, ax);
+                ay = __ffma2_rn(ey, ff, ay);
+                az = __ffma2_rn(ez, ff, az);
+                pt = __fadd2_rn(pt, mr);
+              }
+              if (DBG && me) npair += k - (jself < k ? 1 : 0);
+            } else {
+              for (uint32_t j = 0; j < k; j += 2) {
+                const float2 jx = *reinterpret_cast<const float2*>(&S.lx[j]);
+                const float2 jy = *reinterpret_cast<const float2*>(&S.ly[j]);
+                const float2 jz = *reinterpret_cast<const float2*>(&S.lz[j]);
+                const float2 jm = *reinterpret_cast<const float2*>(&S.lm[j]);
+                const float2 ex = __fadd2_rn(jx, px), ey = __fadd2_rn(jy, py), ez = __fadd2_rn(jz, pz);
+                const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __ffma2_rn(ez, ez, f2(eps2))));
+                const bool u0 = me && j != jself;
+                const bool u1 = me && j + 1 < k && j + 1 != jself;
+                const float2 ri = make_float2(u0 ? rsqrtf(e2.x) : 0.0f, u1 ? rsqrtf(e2.y) : 0.0f);
+                const float2 mr = __fmul2_rn(jm, ri);
+                const float2 ff = __fmul2_rn(__fmul2_rn(mr, ri), ri);
+                ax = __ffma2_rn(ex, ff, ax);
+                ay = __ffma2_rn(ey, ff, ay);
+                az = __ffma2_rn(ez, ff, az);
+                pt = __fadd2_rn(pt, mr);
+                if (DBG) npair += u0 + u1;
+              }
+            }
+          }
         }
-        if (lane == sp) {
-          s_start = w.child;
-          s_cnt = cnt;
-          s_mask = open;
-        }
-        sp++;
       }
     }
-  }
+    if (soft && selfw != 0.0f) pt.x -= selfw * p0.w * rsqrtf(eps2);
 
-  double e_diag = 0, e_true = 0, mx = 0, my = 0, mz = 0, ms = 0;
-  if (valid) {
-    const float G = P.G;
-    ax *= G;
-    ay *= G;
-    az *= G;
-    pot *= G;
-    if (DBG) {
-      a.dbg_acc[i] = make_float4(ax, ay, az, pot);
-      a.dbg_dens[i] = dens;
+    double e_diag = 0, e_true = 0, mx = 0, my = 0, mz = 0, ms = 0;
+    if (valid) {
+      const float G = P.G;
+      float fx = (ax.x + ax.y) * G, fy = (ay.x + ay.y) * G, fz = (az.x + az.y) * G;
+      const float pot = -(pt.x + pt.y) * G;
+      if (DBG) {
+        a.dbg_acc[i] = make_float4(fx, fy, fz, pot);
+        a.dbg_dens[i] = dens;
+      }
+      // Hernquist halo(s), nbody_bh.wgsl:147-157
+      float potHalo = 0.0f;
+      if (P.haloMass > 0.0f) {
+        for (uint32_t h = 0; h < P.haloCount && h < 2; h++) {
+          const float* cc = h == 0 ? P.haloC1 : P.haloC2;
+          const float dx = p0.x - cc[0], dy = p0.y - cc[1], dz = p0.z - cc[2];
+          const float rlen = fmaxf(sqrtf(dx * dx + dy * dy + dz * dz), 1e-6f);
+          const float ra = rlen + P.haloA;
+          const float k = G * P.haloMass / (ra * ra * rlen);
+          fx -= dx * k;
+          fy -= dy * k;
+          fz -= dz * k;
+          potHalo -= G * P.haloMass / ra;
+        }
+      }
+      // kick (nbody_bh.wgsl:161), gas drag (:166-171), drift (:173)
+      float vx = fmaf(fx, P.dt, p1.x), vy = fmaf(fy, P.dt, p1.y), vz = fmaf(fz, P.dt, p1.z);
+      const bool gas = p1.w < -0.5f;
+      if (gas && P.gasDrag > 0.0f) {
+        const float hx = -p0.y, hy = p0.x, hz = 1e-6f;
+        const float il = rsqrtf(hx * hx + hy * hy + hz * hz);
+        const float ux = hx * il, uy = hy * il, uz = hz * il;
+        const float vp = vx * ux + vy * uy + vz * uz;
+        const float damp = expf(-P.gasDrag * P.dt);
+        const float qx = vp * ux, qy = vp * uy, qz = vp * uz;
+        vx = qx + (vx - qx) * damp;
+        vy = qy + (vy - qy) * damp;
+        vz = qz + (vz - qz) * damp;
+      }
+      const float4 o0 = make_float4(fmaf(vx, P.dt, p0.x), fmaf(vy, P.dt, p0.y), fmaf(vz, P.dt, p0.z), p0.w);
+      float4 o1 = make_float4(vx, vy, vz, gas ? -(1.0f + dens) : 0.0f);
+      const float e = 0.5f * (vx * vx + vy * vy + vz * vz) + 0.5f * pot + potHalo;
+      a.energy[i] = e;
+      const double m = p0.w;
+      e_diag = e;
+      e_true = m * (double)e;
+      mx = m * vx;
+      my = m * vy;
+      mz = m * vz;
+      ms = m;
+      if (SF) {
+        float4 s = a.stellar[i];
+        const float4 s_old = s;
+        star_formation_one(P, i, o1, s);
+        if (s.x != s_old.x || s.y != s_old.y || s.z != s_old.z || s.w != s_old.w) a.stellar[i] = s;
+      }
+      a.pout[2 * (size_t)i] = o0;
+      a.pout[2 * (size_t)i + 1] = o1;
     }
-    // Hernquist halo(s), nbody_bh.wgsl:147-157
-    float potHalo = 0.0f;
-    if (P.haloMass > 0.0f) {
-      for (uint32_t h = 0; h < P.haloCount && h < 2; h++) {
-        const float* cc = h == 0 ? P.haloC1 : P.haloC2;
-        const float dx = p0.x - cc[0], dy = p0.y - cc[1], dz = p0.z - cc[2];
-        const float rlen = fmaxf(sqrtf(dx * dx + dy * dy + dz * dz), 1e-6f);
-        const float ra = rlen + P.haloA;
-        const float k = G * P.haloMass / (ra * ra * rlen);
-        ax -= dx * k;
-        ay -= dy * k;
-        az -= dz * k;
-        potHalo -= G * P.haloMass / ra;
+    // per-group partial sums of the diagnostics (fixed order, no atomics)
+    double v[kPartials] = {e_diag, e_true, mx, my, mz, ms};
+#pragma unroll
+    for (int k = 0; k < kPartials; k++) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(full, v[k], o);
+    }
+    if (lane < kPartials) {
+      double mine = v[0];
+#pragma unroll
+      for (int k = 1; k < kPartials; k++)
+        if (lane == k) mine = v[k];
+      a.partials[(size_t)g * kPartials + lane] = mine;
+    }
+    if (DBG) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        nmono += __shfl_xor_sync(full, nmono, o);
+        npair += __shfl_xor_sync(full, npair, o);
+        nvisit += __shfl_xor_sync(full, nvisit, o);
+      }
+      if (lane == 0) {
+        atomicAdd(&a.st->counters[0], nmono);
+        atomicAdd(&a.st->counters[1], npair);
+        atomicAdd(&a.st->counters[2], nvisit);
       }
     }
-    // kick (nbody_bh.wgsl:161), gas drag (:166-171), drift (:173)
-    float vx = fmaf(ax, P.dt, p1.x), vy = fmaf(ay, P.dt, p1.y), vz = fmaf(az, P.dt, p1.z);
-    const bool gas = p1.w < -0.5f;
-    if (gas && P.gasDrag > 0.0f) {
-      const float hx = -p0.y, hy = p0.x, hz = 1e-6f;
-      const float il = rsqrtf(hx * hx + hy * hy + hz * hz);
-      const float ux = hx * il, uy = hy * il, uz = hz * il;
-      const float vp = vx * ux + vy * uy + vz * uz;
-      const float damp = expf(-P.gasDrag * P.dt);
-      const float px = vp * ux, py = vp * uy, pz = vp * uz;
-      vx = px + (vx - px) * damp;
-      vy = py + (vy - py) * damp;
-      vz = pz + (vz - pz) * damp;
-    }
-    float4 o0 = make_float4(fmaf(vx, P.dt, p0.x), fmaf(vy, P.dt, p0.y), fmaf(vz, P.dt, p0.z), p0.w);
-    float4 o1 = make_float4(vx, vy, vz, gas ? -(1.0f + dens) : 0.0f);
-    const float e = 0.5f * (vx * vx + vy * vy + vz * vz) + 0.5f * pot + potHalo;
-    a.energy[i] = e;
-    const double m = p0.w;
-    e_diag = e;
-    e_true = m * ((double)e);
-    mx = m * vx;
-    my = m * vy;
-    mz = m * vz;
-    ms = m;
-    if (SF) {
-      float4 s = a.stellar[i];
-      const float4 s_old = s;
-      star_formation_one(P, i, o1, s);
-      if (s.x != s_old.x || s.y != s_old.y || s.z != s_old.z || s.w != s_old.w) a.stellar[i] = s;
-    }
-    a.pout[2 * (size_t)i] = o0;
-    a.pout[2 * (size_t)i + 1] = o1;
   }
-  // block partial sums of the diagnostics (fixed order, no atomics)
-  double v[kPartials] = {e_diag, e_true, mx, my, mz, ms};
-#pragma unroll
-  for (int k = 0; k < kPartials; k++) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
-    if (lane == 0) s_part[warp][k] = v[k];
-  }
-  if (DBG) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      nmono += __shfl_xor_sync(0xffffffffu, nmono, o);
-      npair += __shfl_xor_sync(0xffffffffu, npair, o);
-      nvisit += __shfl_xor_sync(0xffffffffu, nvisit, o);
+  // the last warp to finish resets the work counters for the next launch
+  if (lane == 0) {
+    const unsigned total = gridDim.x * kWalkWarps;
+    __threadfence();
+    if (atomicAdd(&a.work[1], 1u) == total - 1) {
+      a.work[0] = 0;
+      a.work[1] = 0;
     }
-    if (lane == 0) {
-      atomicAdd(&a.st->counters[0], nmono);
-      atomicAdd(&a.st->counters[1], npair);
-      atomicAdd(&a.st->counters[2], nvisit);
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x < kPartials) {
-    double s = 0;
-    for (int w = 0; w < kWalkWarps; w++) s += s_part[w][threadIdx.x];
-    a.partials[(size_t)blockIdx.x * kPartials + threadIdx.x] = s;
   }
 }
 
