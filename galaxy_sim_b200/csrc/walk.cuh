@@ -30,7 +30,14 @@ constexpr int kWalkThreads = 128;
 constexpr int kWalkWarps = kWalkThreads / 32;
 constexpr int kPartials = 6;  // e_diag, e_true, px, py, pz, mass
 constexpr int kWalkStack = 96;  // ranges; a range push per opened node, <= 7 * depth + 1
-constexpr int kWalkBlocksPerSM = 8;
+#ifndef GS_WALK_BLOCKS_PER_SM
+#define GS_WALK_BLOCKS_PER_SM 8
+#endif
+#ifndef GS_WALK_CHUNK
+#define GS_WALK_CHUNK 1
+#endif
+constexpr int kWalkBlocksPerSM = GS_WALK_BLOCKS_PER_SM;
+constexpr uint32_t kWalkChunk = GS_WALK_CHUNK;  // consecutive groups per grab: L1 reuse
 
 // nbody_bh.wgsl:206-213
 __device__ inline uint32_t pcg(uint32_t v0) {
@@ -105,12 +112,71 @@ struct WalkArgs {
 // Per-warp shared staging.
 struct WalkSmem {
   uint2 stack[kWalkStack];          // {first child | (count-1) << 29, lane mask}
-  float cx[10], cy[10], cz[10], cmass[10], cs2[10];
-  uint4 cmeta[10];                  // {child, info, own-leaf density bits, 0}
-  float lx[34], ly[34], lz[34], lm[34];
+  float cx[8], cy[8], cz[8], cmass[8], cs2[8];
+  uint4 cmeta[8];                   // {child, info, own-leaf density bits, massive}
+  float lx[66], ly[66], lz[66], lm[66];
+  uint4 bl[4];                      // leaf batch: {first particle, count, lane mask, 0}
 };
 
+// Direct sum of a staged leaf segment [off, off + k) for the lanes in `me`
+// (nbody_bh.wgsl:117-131), two sources per packed step. With soft (eps^2 > 0)
+// the self pair is included (zero force at r = 0) and its potential removed
+// once at the end of the walk via selfw; otherwise it is skipped per pair.
+template <typename Smem>
+__device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k, uint32_t jself,
+                                         bool me, bool soft, float2 px, float2 py, float2 pz,
+                                         float eps2, float2& ax, float2& ay, float2& az,
+                                         float2& pt, float& selfw, unsigned long long& npair,
+                                         bool dbg) {
+  if (soft) {
+    const float2 wme = make_float2(me ? 1.0f : 0.0f, me ? 1.0f : 0.0f);
+    if (me && jself < k) selfw += 1.0f;
+    for (uint32_t j = 0; j < k; j += 2) {
+      const float2 jx = *reinterpret_cast<const float2*>(&S.lx[off + j]);
+      const float2 jy = *reinterpret_cast<const float2*>(&S.ly[off + j]);
+      const float2 jz = *reinterpret_cast<const float2*>(&S.lz[off + j]);
+      const float2 jm = *reinterpret_cast<const float2*>(&S.lm[off + j]);
+      const float2 ex = __fadd2_rn(jx, px), ey = __fadd2_rn(jy, py), ez = __fadd2_rn(jz, pz);
+      const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __ffma2_rn(ez, ez, make_float2(eps2, eps2))));
+      const float2 ri = __fmul2_rn(make_float2(rsqrtf(e2.x), rsqrtf(e2.y)), wme);
+      const float2 mr = __fmul2_rn(jm, ri);
+      const float2 ff = __fmul2_rn(__fmul2_rn(mr, ri), ri);
+      ax = __ffma2_rn(ex, ff, ax);
+      ay = __ffma2_rn(ey, ff, ay);
+      az = __ffma2_rn(ez, ff, az);
+      pt = __fadd2_rn(pt, mr);
+    }
+    if (dbg && me) npair += k - (jself < k ? 1 : 0);
+  } else {
+    for (uint32_t j = 0; j < k; j += 2) {
+      const float2 jx = *reinterpret_cast<const float2*>(&S.lx[off + j]);
+      const float2 jy = *reinterpret_cast<const float2*>(&S.ly[off + j]);
+      const float2 jz = *reinterpret_cast<const float2*>(&S.lz[off + j]);
+      const float2 jm = *reinterpret_cast<const float2*>(&S.lm[off + j]);
+      const float2 ex = __fadd2_rn(jx, px), ey = __fadd2_rn(jy, py), ez = __fadd2_rn(jz, pz);
+      const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __ffma2_rn(ez, ez, make_float2(eps2, eps2))));
+      const bool u0 = me && j != jself;
+      const bool u1 = me && j + 1 < k && j + 1 != jself;
+      const float2 ri = make_float2(u0 ? rsqrtf(e2.x) : 0.0f, u1 ? rsqrtf(e2.y) : 0.0f);
+      const float2 mr = __fmul2_rn(jm, ri);
+      const float2 ff = __fmul2_rn(__fmul2_rn(mr, ri), ri);
+      ax = __ffma2_rn(ex, ff, ax);
+      ay = __ffma2_rn(ey, ff, ay);
+      az = __ffma2_rn(ez, ff, az);
+      pt = __fadd2_rn(pt, mr);
+      if (dbg) npair += u0 + u1;
+    }
+  }
+}
+
 __device__ inline float2 f2(float a) { return make_float2(a, a); }
+
+// 1.0f if a > b else 0.0f (ordered compare: NaN gives 0), as one compare-and-set.
+__device__ inline float set_gt(float a, float b) {
+  float r;
+  asm("set.gt.f32.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+  return r;
+}
 
 __device__ inline void prefetch_l1(const void* p) {
   asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
@@ -129,12 +195,18 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
   const uint32_t ngroups = (a.N + 31) / 32;
   const unsigned full = 0xffffffffu;
 
+  uint32_t g = 0, gstop = 0;
   while (true) {
-    uint32_t g = 0;
-    if (lane == 0) g = atomicAdd(&a.work[0], 1u);
-    g = __shfl_sync(full, g, 0);
-    if (g >= ngroups) break;
-    const uint32_t gbeg = g * 32, gend = gbeg + 32;
+    if (g == gstop) {  // grab the next chunk of consecutive groups
+      uint32_t c = 0;
+      if (lane == 0) c = atomicAdd(&a.work[0], 1u);
+      c = __shfl_sync(full, c, 0);
+      g = c * kWalkChunk;
+      gstop = min(g + kWalkChunk, ngroups);
+      if (g >= ngroups) break;
+    }
+    const uint32_t gcur = g++;
+    const uint32_t gbeg = gcur * 32, gend = gbeg + 32;
     const uint32_t i = gbeg + lane;
     const bool valid = i < a.N;
     float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0;
@@ -163,10 +235,13 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
         break;
       }
       __syncwarp();
-      // stage the range: one child per lane, plus a massless partner for an odd count
+      // Stage the range in lanes 0..7: one child per lane; lanes past the count hold
+      // massless dummies. Massless and sub-softening children (size^2 < eps^2/4,
+      // always accepted, nbody_bh.wgsl:112) get size^2 = -inf, so the per-lane test
+      // is the single compare size^2 < theta^2 (r^2 + eps^2).
       bool own = false;
-      if (lane <= (int)cnt) {
-        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (lane < 8) {
+        float4 q = make_float4(1e30f, 1e30f, 1e30f, 0.f);
         WalkInfo w;
         w.s2 = 0.f;
         w.child = 0;
@@ -177,19 +252,34 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
           w = a.info[start + lane];
         }
         const uint32_t wc = w.info & ~kLeafBit;
-        own = (w.info & kLeafBit) && q.w != 0.0f && w.child < gend && w.child + wc > gbeg;
+        own = lane < (int)cnt && (w.info & kLeafBit) && q.w != 0.0f && w.child < gend &&
+              w.child + wc > gbeg;
+        float s2 = w.s2;
+        if (q.w == 0.0f) {  // never opened, contributes nothing (far away, massless)
+          s2 = -INFINITY;
+          q = make_float4(1e30f, 1e30f, 1e30f, 0.f);
+        } else if (s2 < qe2) {
+          s2 = -INFINITY;
+        }
         S.cx[lane] = q.x;
         S.cy[lane] = q.y;
         S.cz[lane] = q.z;
         S.cmass[lane] = q.w;
-        S.cs2[lane] = w.s2;
+        S.cs2[lane] = s2;
         S.cmeta[lane] = make_uint4(w.child, w.info,
-                                   own ? __float_as_uint((float)wc / (w.size * w.size * w.size)) : 0u, 0u);
+                                   own ? __float_as_uint((float)wc / (w.size * w.size * w.size)) : 0u,
+                                   q.w != 0.0f ? 1u : 0u);
       }
-      const unsigned ownmask = __ballot_sync(full, own);  // leaves holding this warp's particles
+      const unsigned ownmask = __ballot_sync(full, own) & 0xffu;  // leaves holding our particles
+      const unsigned leafmask = __ballot_sync(full, lane < (int)cnt && (S.cmeta[lane & 7].y & kLeafBit)) & 0xffu;
+      const unsigned massmask = DBG ? (__ballot_sync(full, lane < (int)cnt && S.cmeta[lane & 7].w) & 0xffu) : 0u;
       __syncwarp();
       const bool act = (mask >> lane) & 1u;
-      for (uint32_t c = 0; c < cnt; c += 2) {
+      const float2 actw = f2(act ? 1.0f : 0.0f);
+      float2 wt[4];  // accept weights (1.0 / 0.0) of children 2p, 2p+1
+#pragma unroll
+      for (int pp = 0; pp < 4; pp++) {
+        const int c = 2 * pp;
         const float2 qx = *reinterpret_cast<const float2*>(&S.cx[c]);
         const float2 qy = *reinterpret_cast<const float2*>(&S.cy[c]);
         const float2 qz = *reinterpret_cast<const float2*>(&S.cz[c]);
@@ -198,120 +288,120 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
         const float2 rx = __fadd2_rn(qx, px), ry = __fadd2_rn(qy, py), rz = __fadd2_rn(qz, pz);
         const float2 d2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __ffma2_rn(rz, rz, f2(eps2))));
         const float2 td = __fmul2_rn(f2(theta2), d2);
-        const bool live0 = act && qm.x != 0.0f, live1 = act && qm.y != 0.0f;
-        const bool ok0 = (s2.x < td.x) || (s2.x < qe2);
-        const bool ok1 = (s2.y < td.y) || (s2.y < qe2);
-        const bool acc0 = live0 && ok0, acc1 = live1 && ok1;
-        const float2 rinv = make_float2(acc0 ? rsqrtf(d2.x) : 0.0f, acc1 ? rsqrtf(d2.y) : 0.0f);
+        const float2 w = __fmul2_rn(make_float2(set_gt(td.x, s2.x), set_gt(td.y, s2.y)), actw);
+        wt[pp] = w;
+        const float2 rinv = __fmul2_rn(make_float2(rsqrtf(d2.x), rsqrtf(d2.y)), w);
         const float2 mr = __fmul2_rn(qm, rinv);
         const float2 f = __fmul2_rn(__fmul2_rn(mr, rinv), rinv);
         ax = __ffma2_rn(rx, f, ax);
         ay = __ffma2_rn(ry, f, ay);
         az = __ffma2_rn(rz, f, az);
         pt = __fadd2_rn(pt, mr);  // sum of m/r; potential = -G * sum
-        if (DBG) {
-          nmono += acc0 + acc1;
-          nvisit += live0 + live1;
-        }
-        // own-leaf density (nbody_bh.wgsl:93-95): only leaves that hold this warp's particles
-        if ((ownmask >> c) & 3u) {
+      }
+      // bitmask of the children this lane opens (active, accept weight 0)
+      uint32_t obits = 0;
 #pragma unroll
-          for (int h = 0; h < 2; h++) {
-            if (!((ownmask >> (c + h)) & 1u)) continue;
-            const uint4 mt = S.cmeta[c + h];
-            if ((h ? live1 : live0) && (i - mt.x) < (mt.y & ~kLeafBit)) dens = __uint_as_float(mt.z);
-          }
+      for (int pp = 0; pp < 4; pp++) {
+        obits |= (wt[pp].x == 0.0f ? 1u : 0u) << (2 * pp);
+        obits |= (wt[pp].y == 0.0f ? 1u : 0u) << (2 * pp + 1);
+      }
+      obits = act ? (obits & ((1u << cnt) - 1u)) : 0u;
+      const uint32_t om = __reduce_or_sync(full, obits);  // children opened by some lane
+      if (DBG && act) {
+        const uint32_t real = __popc(massmask & ((1u << cnt) - 1u));
+        nvisit += real;
+        nmono += real - __popc(obits);
+      }
+      for (uint32_t bb = ownmask; bb; bb &= bb - 1) {  // own-leaf density (nbody_bh.wgsl:93-95)
+        const uint4 mt = S.cmeta[__ffs(bb) - 1];
+        if (act && (i - mt.x) < (mt.y & ~kLeafBit)) dens = __uint_as_float(mt.z);
+      }
+      if (!om) continue;
+      // opened internal children: push their child ranges
+      for (uint32_t bb = om & ~leafmask; bb; bb &= bb - 1) {
+        const uint32_t cc = __ffs(bb) - 1;
+        const unsigned open = __ballot_sync(full, (obits >> cc) & 1u);
+        const uint4 mt = S.cmeta[cc];
+        const uint32_t cchild = mt.x, ccnt = mt.y & ~kLeafBit;
+        if (!(cchild > start + cc && (uint64_t)cchild + ccnt <= a.node_cap && ccnt >= 1u && ccnt <= 8u)) {
+          if (lane == 0) raise_err(a.st, GS_DERR_TREE);
+          continue;
         }
-        const bool op0 = live0 && !ok0, op1 = live1 && !ok1;
-        if (!__ballot_sync(full, op0 || op1)) continue;
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-          const uint32_t cc = c + h;
-          const unsigned open = __ballot_sync(full, h ? op1 : op0);
-          if (!open) continue;
+        if (sp >= kWalkStack) {  // cannot happen for depth <= 10 trees
+          if (lane == 0) raise_err(a.st, GS_DERR_STACK);
+          continue;
+        }
+        if (lane == 0) S.stack[sp] = make_uint2(cchild | ((ccnt - 1u) << 29), open);
+        if (lane < (int)ccnt) {  // warm L1 for the range's staging load
+          prefetch_l1(&a.cm[cchild + lane]);
+          prefetch_l1(&a.info[cchild + lane]);
+        }
+        sp++;
+      }
+      // opened leaves: direct sums, two sources at a time; leaves of <= 16
+      // particles are staged four per batch (one load round), larger ones in chunks
+      uint32_t small = 0, big = 0;
+      for (uint32_t bb = om & leafmask; bb; bb &= bb - 1) {
+        const uint32_t cc = __ffs(bb) - 1;
+        const uint4 mt = S.cmeta[cc];
+        const uint32_t ccnt = mt.y & ~kLeafBit;
+        if ((uint64_t)mt.x + ccnt > a.N) {
+          if (lane == 0) raise_err(a.st, GS_DERR_TREE);
+          continue;
+        }
+        if (ccnt > 16u) big |= 1u << cc;
+        else small |= 1u << cc;
+      }
+      while (small) {
+        uint32_t nb = 0;
+        __syncwarp();
+        while (small && nb < 4) {
+          const uint32_t cc = __ffs(small) - 1;
+          small &= small - 1;
+          const unsigned open = __ballot_sync(full, (obits >> cc) & 1u);
           const uint4 mt = S.cmeta[cc];
-          const uint32_t cchild = mt.x;
-          const bool leaf = (mt.y & kLeafBit) != 0u;
-          const uint32_t ccnt = mt.y & ~kLeafBit;
-          const bool sane = leaf ? ((uint64_t)cchild + ccnt <= a.N)
-                                 : (cchild > start + cc && (uint64_t)cchild + ccnt <= a.node_cap &&
-                                    ccnt >= 1u && ccnt <= 8u);
-          if (!sane) {
-            if (lane == 0) raise_err(a.st, GS_DERR_TREE);
-            continue;
+          if (lane == 0) S.bl[nb] = make_uint4(mt.x, mt.y & ~kLeafBit, open, 0u);
+          nb++;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+          const uint32_t e = lane + 32 * r, slot = e >> 4, q = e & 15u;
+          if (slot < nb) {
+            const uint4 bl = S.bl[slot];
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (q < bl.y) v = __ldg(&a.pin[2 * (size_t)(bl.x + q)]);
+            S.lx[e] = v.x;
+            S.ly[e] = v.y;
+            S.lz[e] = v.z;
+            S.lm[e] = v.w;
           }
-          if (!leaf) {
-            if (sp >= kWalkStack) {  // cannot happen for depth <= 10 trees
-              if (lane == 0) raise_err(a.st, GS_DERR_STACK);
-              continue;
-            }
-            if (lane == 0) S.stack[sp] = make_uint2(cchild | ((ccnt - 1u) << 29), open);
-            if (lane < (int)ccnt) {  // warm L1 for the range's staging load
-              prefetch_l1(&a.cm[cchild + lane]);
-              prefetch_l1(&a.info[cchild + lane]);
-            }
-            sp++;
-            continue;
-          }
-          // leaf direct sum over [cchild, cchild + ccnt), two sources at a time
-          const bool me = (open >> lane) & 1u;
-          const float2 wme = f2(me ? 1.0f : 0.0f);
-          for (uint32_t b0 = 0; b0 < ccnt; b0 += 32) {
-            const uint32_t k = min(32u, ccnt - b0);
-            __syncwarp();
-            if (lane < (int)k) {
-              const float4 q = __ldg(&a.pin[2 * (size_t)(cchild + b0 + lane)]);
-              S.lx[lane] = q.x;
-              S.ly[lane] = q.y;
-              S.lz[lane] = q.z;
-              S.lm[lane] = q.w;
-            } else if (lane == (int)k) {
-              S.lx[lane] = S.ly[lane] = S.lz[lane] = 0.f;
-              S.lm[lane] = 0.f;
-            }
-            __syncwarp();
-            const uint32_t jself = i - (cchild + b0);  // my own slot, if in this chunk
-            if (soft) {
-              // every pair incl. j == i (zero force at r = 0); the self potential
-              // m_i / eps is removed once at the end
-              if (me && jself < k) selfw += 1.0f;
-              for (uint32_t j = 0; j < k; j += 2) {
-                const float2 jx = *reinterpret_cast<const float2*>(&S.lx[j]);
-                const float2 jy = *reinterpret_cast<const float2*>(&S.ly[j]);
-                const float2 jz = *reinterpret_cast<const float2*>(&S.lz[j]);
-                const float2 jm = *reinterpret_cast<const float2*>(&S.lm[j]);
-                const float2 ex = __fadd2_rn(jx, px), ey = __fadd2_rn(jy, py), ez = __fadd2_rn(jz, pz);
-                const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __ffma2_rn(ez, ez, f2(eps2))));
-                const float2 ri = __fmul2_rn(make_float2(rsqrtf(e2.x), rsqrtf(e2.y)), wme);
-                const float2 mr = __fmul2_rn(jm, ri);
-                const float2 ff = __fmul2_rn(__fmul2_rn(mr, ri), ri);
-                ax = __ffma2_rn(ex, ff, ax);
-                ay = __ffma2_rn(ey, ff, ay);
-                az = __ffma2_rn(ez, ff, az);
-                pt = __fadd2_rn(pt, mr);
-              }
-              if (DBG && me) npair += k - (jself < k ? 1 : 0);
-            } else {
-              for (uint32_t j = 0; j < k; j += 2) {
-                const float2 jx = *reinterpret_cast<const float2*>(&S.lx[j]);
-                const float2 jy = *reinterpret_cast<const float2*>(&S.ly[j]);
-                const float2 jz = *reinterpret_cast<const float2*>(&S.lz[j]);
-                const float2 jm = *reinterpret_cast<const float2*>(&S.lm[j]);
-                const float2 ex = __fadd2_rn(jx, px), ey = __fadd2_rn(jy, py), ez = __fadd2_rn(jz, pz);
-                const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __ffma2_rn(ez, ez, f2(eps2))));
-                const bool u0 = me && j != jself;
-                const bool u1 = me && j + 1 < k && j + 1 != jself;
-                const float2 ri = make_float2(u0 ? rsqrtf(e2.x) : 0.0f, u1 ? rsqrtf(e2.y) : 0.0f);
-                const float2 mr = __fmul2_rn(jm, ri);
-                const float2 ff = __fmul2_rn(__fmul2_rn(mr, ri), ri);
-                ax = __ffma2_rn(ex, ff, ax);
-                ay = __ffma2_rn(ey, ff, ay);
-                az = __ffma2_rn(ez, ff, az);
-                pt = __fadd2_rn(pt, mr);
-                if (DBG) npair += u0 + u1;
-              }
-            }
-          }
+        }
+        __syncwarp();
+        for (uint32_t sl = 0; sl < nb; sl++) {
+          const uint4 bl = S.bl[sl];
+          leaf_sum(S, 16 * sl, bl.y, i - bl.x, (bl.z >> lane) & 1u, soft, px, py, pz, eps2, ax, ay,
+                   az, pt, selfw, npair, DBG);
+        }
+      }
+      for (uint32_t bb = big; bb; bb &= bb - 1) {
+        const uint32_t cc = __ffs(bb) - 1;
+        const unsigned open = __ballot_sync(full, (obits >> cc) & 1u);
+        const uint4 mt = S.cmeta[cc];
+        const uint32_t cchild = mt.x, ccnt = mt.y & ~kLeafBit;
+        for (uint32_t b0 = 0; b0 < ccnt; b0 += 32) {
+          const uint32_t k = min(32u, ccnt - b0);
+          __syncwarp();
+          float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (lane < (int)k) v = __ldg(&a.pin[2 * (size_t)(cchild + b0 + lane)]);
+          S.lx[lane] = v.x;
+          S.ly[lane] = v.y;
+          S.lz[lane] = v.z;
+          S.lm[lane] = v.w;
+          if (lane == 0) S.lx[32] = S.ly[32] = S.lz[32] = S.lm[32] = 0.f;
+          __syncwarp();
+          leaf_sum(S, 0, k, i - (cchild + b0), (open >> lane) & 1u, soft, px, py, pz, eps2, ax, ay,
+                   az, pt, selfw, npair, DBG);
         }
       }
     }
@@ -387,7 +477,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
 #pragma unroll
       for (int k = 1; k < kPartials; k++)
         if (lane == k) mine = v[k];
-      a.partials[(size_t)g * kPartials + lane] = mine;
+      a.partials[(size_t)gcur * kPartials + lane] = mine;
     }
     if (DBG) {
 #pragma unroll
