@@ -89,6 +89,7 @@ SIGNATURES = [
     ("gs_tree_build", _int, [_vp, _vp, _vp, _u32, _f64, _u32, _vp, _vp, _vp, _u32, _vp]),
     ("gs_sort_and_build", _int, [_vp, _vp, _u32, _i64, _vp, _vp, _vp, _vp, _u32, _vp, _vp, _u32,
                                  _vp, _vp, _vp, _vp]),
+    ("gs_radix_sort_indices_noalloc", _int, [_vp, _u32, _vp, _vp]),
 ]
 
 _lib = None

@@ -1,6 +1,7 @@
 """Build the in-tree CUDA library ``libgalaxy_b200.so`` for sm_100a.
 
-Compiles ``csrc/galaxy_b200.cu`` (which includes every kernel header) with
+Compiles ``csrc/galaxy_b200.cu`` (which includes every kernel header) and
+``csrc/noalloc.cu`` with
 nvcc for ``compute_100a``/``sm_100a`` only, position-independent, into the
 package directory so the library travels with the source tree.
 """
@@ -47,8 +48,8 @@ def up_to_date() -> bool:
 def build(force: bool = False, verbose: bool = False, extra=()) -> str:
     if not force and up_to_date():
         return LIB
-    cmd = [nvcc(), *NVCC_FLAGS, *extra, "-I", INCLUDE, "-o", LIB + ".tmp",
-           os.path.join(CSRC, "galaxy_b200.cu")]
+    units = [os.path.join(CSRC, f) for f in ("galaxy_b200.cu", "noalloc.cu")]
+    cmd = [nvcc(), *NVCC_FLAGS, *extra, "-I", INCLUDE, "-o", LIB + ".tmp", *units]
     env = dict(os.environ)
     # nvcc needs a host compiler it supports; the system g++ is one
     if os.path.exists("/usr/bin/g++"):

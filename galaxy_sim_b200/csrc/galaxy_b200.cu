@@ -409,6 +409,13 @@ int host_pack4(const float* src, uint32_t N, uint32_t stride, std::vector<float4
 extern "C" {
 
 const char* gs_last_error(const gs_ctx* ctx) { return ctx ? ctx->err : g_err; }
+
+}  // extern "C"
+
+// Context-free error text for entry points defined in other translation units.
+void gs_internal_set_error(const char* msg) { set_err(g_err, "%s", msg); }
+
+extern "C" {
 const char* gs_version(void) { return "galaxy_b200 0.1 (sm_100a)"; }
 
 int gs_device_count(int* count) {

@@ -1,0 +1,155 @@
+// Allocation-free stable radix sort: gs_radix_sort_indices_noalloc.
+//
+// Some callers may not allocate device memory once they are running: a host
+// application's per-frame callback (cudaMalloc and cudaFree can synchronize the
+// whole device and stall its other streams mid-frame), or an embedding engine
+// that budgets device memory at start-up and forbids allocation afterwards.
+// This variant of the sort behind gs_radix_sort_indices allocates nothing. The
+// caller passes device pointers for the codes and the permutation, plus the
+// stream to run on. Every intermediate buffer lives in one file-scope static
+// device array sized for at most kNoAllocMaxN codes. Each GPU that loads the
+// library holds that array until the process exits.
+//
+// The host code never hands the array's name to a kernel. In host code that
+// name only stands in for the device object, so a kernel given it would fault
+// or, where the GPU can reach host memory, silently use the wrong memory. The
+// first call on each device (with that device current) looks up the array's
+// device address with cudaGetSymbolAddress and caches it. That first call
+// should come before any stream capture.
+//
+// All calls share the one array, and it keeps the contents of the last call.
+// Each call therefore clears the histograms, tile counters and look-back
+// words it relies on before using them. Calls whose work overlaps on the GPU
+// (two streams, or two host threads) race on that shared array: serialize them.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <mutex>
+
+#include "common.cuh"
+#include "sort.cuh"
+
+void gs_internal_set_error(const char* msg);
+
+namespace {
+
+using namespace gs;
+
+constexpr uint32_t kNoAllocMaxN = 1u << 20;  // 1,048,576 codes
+constexpr uint32_t kNoAllocTiles = (kNoAllocMaxN + kSortTile - 1) / kSortTile;
+constexpr int kNoAllocPasses = 4;
+// two key buffers + one payload buffer, then histograms | tile counters | look-back
+constexpr size_t kKeyWords = (size_t)kNoAllocMaxN;
+constexpr size_t kHistOff = 3 * kKeyWords;
+constexpr size_t kCtrOff = kHistOff + kNoAllocPasses * 256;
+constexpr size_t kLbOff = kCtrOff + 16;
+constexpr size_t kScratchWords = kLbOff + (size_t)kNoAllocPasses * kNoAllocTiles * 256;
+constexpr size_t kClearBytes = (kScratchWords - kHistOff) * sizeof(uint32_t);
+
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kScratchWords];  // about 13 MiB
+static __device__ DevState g_noalloc_state;                                   // error word
+
+constexpr int kMaxDevices = 64;
+void* g_scratch_addr[kMaxDevices];
+void* g_state_addr[kMaxDevices];
+std::mutex g_setup_mutex;
+
+// radixSortIndices orders by the low 30 bits (mortonTree.js:71-74): copy the
+// masked codes into the first key buffer and count every pass's digits.
+__global__ void noalloc_mask_hist_kernel(const uint32_t* __restrict__ codes, uint32_t N,
+                                         uint32_t* __restrict__ keys, uint32_t* hist) {
+  __shared__ uint32_t s_hist[kNoAllocPasses * 256];
+  for (int k = threadIdx.x; k < kNoAllocPasses * 256; k += blockDim.x) s_hist[k] = 0;
+  __syncthreads();
+  for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < N; i0 += gridDim.x * blockDim.x) {
+    const uint32_t i = i0 + threadIdx.x;
+    const bool valid = i < N;
+    uint32_t key = 0;
+    if (valid) {
+      key = codes[i] & 0x3fffffffu;
+      keys[i] = key;
+    }
+    hist_add_warp(s_hist, key, valid, kNoAllocPasses);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < kNoAllocPasses * 256; k += blockDim.x)
+    if (s_hist[k]) atomicAdd(&hist[k], s_hist[k]);
+}
+
+int fail(int code, const char* msg) {
+  gs_internal_set_error(msg);
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  char buf[256];
+  snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+  gs_internal_set_error(buf);
+  return e == cudaErrorMemoryAllocation ? GS_ENOMEM : GS_ECUDA;
+}
+
+}  // namespace
+
+extern "C" int gs_radix_sort_indices_noalloc(const uint32_t* d_codes, uint32_t N, uint32_t* d_perm,
+                                             void* stream) {
+  if (N == 0) return GS_OK;
+  if (!d_codes || !d_perm) return fail(GS_EINVAL, "d_codes and d_perm must be device pointers");
+  if (N > kNoAllocMaxN)
+    return fail(GS_EINVAL, "gs_radix_sort_indices_noalloc: N exceeds its static scratch "
+                           "(at most 1048576 codes)");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices) return fail(GS_EINVAL, "device ordinal out of range");
+  {
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (!g_scratch_addr[dev]) {  // once per device, with that device current
+      void* p = nullptr;
+      void* q = nullptr;
+      e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(scratch)");
+      e = cudaGetSymbolAddress(&q, g_noalloc_state);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(state)");
+      g_state_addr[dev] = q;
+      g_scratch_addr[dev] = p;
+    }
+  }
+  uint32_t* base = static_cast<uint32_t*>(g_scratch_addr[dev]);
+  DevState* st = static_cast<DevState*>(g_state_addr[dev]);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  uint32_t* k0 = base;
+  uint32_t* k1 = base + kKeyWords;
+  uint32_t* v0 = base + 2 * kKeyWords;
+  uint32_t* hist = base + kHistOff;
+  uint32_t* ctr = base + kCtrOff;
+  uint32_t* lb = base + kLbOff;
+  const uint32_t tiles = (N + kSortTile - 1) / kSortTile;
+  // what must start at zero: histograms, tile counters, look-back words, error word
+  if ((e = cudaMemsetAsync(hist, 0, kClearBytes, s)) != cudaSuccess) return cuda_fail(e, "clear");
+  if ((e = cudaMemsetAsync(&st->err, 0, sizeof(unsigned), s)) != cudaSuccess)
+    return cuda_fail(e, "clear");
+  const uint32_t grid = std::min<uint32_t>(148 * 8, (N + 255) / 256);
+  noalloc_mask_hist_kernel<<<grid, 256, 0, s>>>(d_codes, N, k0, hist);
+  // pass 0: k0 -> k1 (payload = index) -> v0; 1: -> k0, d_perm; 2: -> k1, v0; 3: -> k0, d_perm
+  uint32_t* kin[kNoAllocPasses] = {k0, k1, k0, k1};
+  uint32_t* kout[kNoAllocPasses] = {k1, k0, k1, k0};
+  uint32_t* vin[kNoAllocPasses] = {nullptr, v0, d_perm, v0};
+  uint32_t* vout[kNoAllocPasses] = {v0, d_perm, v0, d_perm};
+  for (int p = 0; p < kNoAllocPasses; p++) {
+    uint32_t* plb = lb + (size_t)p * kNoAllocTiles * 256;
+    if (p == 0)
+      onesweep_pass<true><<<tiles, kSortThreads, 0, s>>>(kin[p], nullptr, kout[p], vout[p],
+                                                         hist + p * 256, plb, ctr + p, N, 8 * p, st);
+    else
+      onesweep_pass<false><<<tiles, kSortThreads, 0, s>>>(kin[p], vin[p], kout[p], vout[p],
+                                                          hist + p * 256, plb, ctr + p, N, 8 * p, st);
+  }
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "sort launch");
+  unsigned err = 0;
+  if ((e = cudaMemcpyAsync(&err, &st->err, sizeof(unsigned), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    return cuda_fail(e, "error word");
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+  if (err) return fail(GS_EDEVICE, "sort look-back wait exceeded its iteration limit");
+  return GS_OK;
+}

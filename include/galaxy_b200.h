@@ -187,6 +187,24 @@ int gs_sort_and_build(const float* particles8, const float* stellar4, uint32_t N
                       uint32_t* level_ranges, uint32_t lr_cap, uint32_t* n_levels,
                       int64_t* central_idx, int64_t* central_idx2, float* sorted_mass);
 
+/* ---- allocation-free sort ------------------------------------------------------------- */
+
+/* No counterpart in the reference. The stable radix sort of gs_radix_sort_indices
+ * (same permutation) for callers that may not allocate device memory while they
+ * run, such as a host's per-frame callback (cudaMalloc/cudaFree can synchronize
+ * the device and stall the frame) or an engine that budgets device memory at
+ * start-up. d_codes (N codes, only the low 30 bits count) and d_perm (N
+ * indices) are device buffers the caller owns; stream is a cudaStream_t (NULL =
+ * the default stream). The call allocates nothing: its scratch is one static
+ * device array for at most 1048576 codes (about 13 MiB), held by every GPU that
+ * loads the library until the process exits; larger N is rejected with
+ * GS_EINVAL. The first call on a device looks up that array's device address and
+ * should come before any stream capture. Calls share the array, so calls whose
+ * work overlaps on the GPU race: serialize them. Returns after the stream has
+ * finished the sort. */
+int gs_radix_sort_indices_noalloc(const uint32_t* d_codes, uint32_t N, uint32_t* d_perm,
+                                  void* stream);
+
 #ifdef __cplusplus
 }
 #endif
