@@ -21,6 +21,8 @@
 #include "common.cuh"
 #include "morton.cuh"
 
+#include <cuda/atomic>
+
 namespace gs {
 
 constexpr int kFlagThreads = 256;
@@ -351,11 +353,12 @@ __global__ void __launch_bounds__(256) tree_leaves_kernel(BuildBuffers b, const 
         if (st) raise_err(st, GS_DERR_NODES);
         break;
       }
-      __threadfence();
-      const uint32_t old = atomicAdd(&b.arrive[p], 1u);
+      // release: this node's COM is visible before the count; acquire: the last
+      // arriver sees every sibling's COM
+      const uint32_t old = cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(b.arrive[p])
+                               .fetch_add(1u, cuda::memory_order_acq_rel);
       if (old + 1 != nc) break;
       b.arrive[p] = 0;
-      __threadfence();
       const uint32_t cb = b.child_base[p];
       float4 pc;
       if (MODE == kComF32) {

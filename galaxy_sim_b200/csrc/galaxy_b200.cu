@@ -474,7 +474,7 @@ int gs_create_on(int device, uint32_t N, const float* particles8, const float* s
   if ((rc = c->cuda(w.alloc(&c->compact, N), "compact"))) return bail(rc);
   if ((rc = c->cuda(w.alloc(&c->perm_user, N), "perm"))) return bail(rc);
   if ((rc = c->cuda(w.alloc(&c->st, 1), "state"))) return bail(rc);
-  c->walk_groups = cdiv(N, 32);
+  c->walk_groups = cdiv(N, kWalkGroup);
   {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);

@@ -11,7 +11,10 @@
 namespace gs {
 
 constexpr int kBBoxThreads = 256;
-constexpr int kBBoxBlocks = 296;  // 2 per SM on a 148-SM B200
+#ifndef GS_BBOX_BLOCKS
+#define GS_BBOX_BLOCKS 1184
+#endif
+constexpr int kBBoxBlocks = GS_BBOX_BLOCKS;  // blocks of the bbox reduction
 
 // Bounding box over finite particles (mortonTree.js:44-52), float min/max
 // as ordered ints; the last block folds the partials, derives the double frame
@@ -59,12 +62,35 @@ __global__ void __launch_bounds__(kBBoxThreads)
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  if (threadIdx.x < 6) {
-    int v = __ldcg(&partials[threadIdx.x]);
-    for (uint32_t b = 1; b < gridDim.x; b++) {
-      const int t = __ldcg(&partials[b * 6 + threadIdx.x]);
-      v = threadIdx.x < 3 ? min(v, t) : max(v, t);
+  // fold the per-block partials with the whole block (independent loads in flight)
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    mn[k] = float_to_ordered(INFINITY);
+    mx[k] = float_to_ordered(-INFINITY);
+  }
+  for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      mn[k] = min(mn[k], __ldcg(&partials[b * 6 + k]));
+      mx[k] = max(mx[k], __ldcg(&partials[b * 6 + 3 + k]));
     }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    mn[k] = __reduce_min_sync(0xffffffffu, mn[k]);
+    mx[k] = __reduce_max_sync(0xffffffffu, mx[k]);
+  }
+  __syncthreads();
+  if (lane == 0)
+    for (int k = 0; k < 3; k++) {
+      s_red[warp][k] = mn[k];
+      s_red[warp][3 + k] = mx[k];
+    }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    int v = s_red[0][threadIdx.x];
+    for (int w = 1; w < kBBoxThreads / 32; w++)
+      v = threadIdx.x < 3 ? min(v, s_red[w][threadIdx.x]) : max(v, s_red[w][threadIdx.x]);
     s_red[0][threadIdx.x] = v;
   }
   __syncthreads();
@@ -102,7 +128,12 @@ __global__ void __launch_bounds__(256)
       code = morton_code(f, p.x, p.y, p.z);
       codes[i] = code;
     }
+#ifndef GS_HIST_MATCH
+    if (hist && valid)
+      for (int p = 0; p < passes; p++) atomicAdd(&s_hist[p * 256 + ((code >> (8 * p)) & 255u)], 1u);
+#else
     if (hist) hist_add_warp(s_hist, code, valid, passes);
+#endif
   }
   if (!hist) return;
   __syncthreads();

@@ -10,7 +10,10 @@ namespace gs {
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortItems = 16;
+#ifndef GS_SORT_ITEMS
+#define GS_SORT_ITEMS 16
+#endif
+constexpr int kSortItems = GS_SORT_ITEMS;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
 constexpr uint32_t kLbAgg = 1u << 30;
 constexpr uint32_t kLbInc = 2u << 30;
@@ -112,19 +115,32 @@ __global__ void __launch_bounds__(kSortThreads)
     excl = 0;
     int64_t t = (int64_t)tile - 1;
     uint32_t spins = 0;
-    while (t >= 0) {
-      const uint32_t v = ld_relaxed(lookback + (size_t)t * 256 + d);
-      const uint32_t flag = v & ~kLbMask;
-      if (flag == 0) {
-        if (++spins > kSpinLimit) {
-          raise_err(st, GS_DERR_LOOKBACK);
+    bool done = false;
+    while (t >= 0 && !done) {
+      // look at up to 32 predecessors at once (independent loads in flight)
+      constexpr int kWin = 32;
+      uint32_t v[kWin];
+#pragma unroll
+      for (int k = 0; k < kWin; k++)
+        v[k] = (t - k >= 0) ? ld_relaxed(lookback + (size_t)(t - k) * 256 + d) : kLbInc;
+      int used = 0;
+#pragma unroll
+      for (int k = 0; k < kWin; k++) {
+        if (used < k) break;  // an earlier entry was not published yet
+        const uint32_t flag = v[k] & ~kLbMask;
+        if (flag == 0) break;  // not published yet: reload from here
+        excl += v[k] & kLbMask;
+        used = k + 1;
+        if (flag == kLbInc) {
+          done = true;
           break;
         }
-        continue;
       }
-      excl += v & kLbMask;
-      if (flag == kLbInc) break;
-      t--;
+      t -= used;
+      if (!done && used == 0 && ++spins > kSpinLimit) {
+        raise_err(st, GS_DERR_LOOKBACK);
+        break;
+      }
     }
     st_relaxed(&lb[d], kLbInc | ((excl + tot) & kLbMask));
   }

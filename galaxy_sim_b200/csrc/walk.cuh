@@ -38,6 +38,7 @@ constexpr int kWalkStack = 96;  // ranges; a range push per opened node, <= 7 * 
 #endif
 constexpr int kWalkBlocksPerSM = GS_WALK_BLOCKS_PER_SM;
 constexpr uint32_t kWalkChunk = GS_WALK_CHUNK;  // consecutive groups per grab: L1 reuse
+constexpr uint32_t kWalkGroup = 32;             // particles per warp (one per lane)
 
 // nbody_bh.wgsl:206-213
 __device__ inline uint32_t pcg(uint32_t v0) {
