@@ -74,6 +74,7 @@ SIGNATURES = [
     ("gs_get_tracking", _int, [_vp, _vp, _vp, _vp, _vp]),
     ("gs_sort_build", _int, [_vp]),
     ("gs_run", _int, [_vp, _u32, _int]),
+    ("gs_step_kernels", _int, [_vp, _vp]),
     ("gs_stream", _int, [_vp, _vp]),
     ("gs_sync", _int, [_vp, C.c_uint64]),
     ("gs_get_tree", _int, [_vp, _vp, _u32, _vp, _vp, _u32, _vp, _vp]),
@@ -89,6 +90,14 @@ SIGNATURES = [
     ("gs_tree_build", _int, [_vp, _vp, _vp, _u32, _f64, _u32, _vp, _vp, _vp, _u32, _vp]),
     ("gs_sort_and_build", _int, [_vp, _vp, _u32, _i64, _vp, _vp, _vp, _vp, _u32, _vp, _vp, _u32,
                                  _vp, _vp, _vp, _vp]),
+    ("gs_device_memory", _int, [_int, _vp, _vp]),
+    ("gs_pool_bytes", C.c_uint64, [C.c_uint64, _u32]),
+    ("gs_pool_create", _int, [_int, C.c_uint64, _u32, _vp]),
+    ("gs_pool_add", _int, [_vp, _u32, _vp, _vp, _vp, _vp]),
+    ("gs_pool_remove", _int, [_vp, _u32]),
+    ("gs_pool_free", _int, [_vp, _vp, _vp]),
+    ("gs_select", _int, [_vp, _u32]),
+    ("gs_pool_energies", _int, [_vp, _vp, _u32]),
     ("gs_radix_sort_indices_noalloc", _int, [_vp, _u32, _vp, _vp]),
 ]
 

@@ -17,6 +17,11 @@
 // The third leaf clause of mortonTree.js:127 (numNodes + 8 > maxNodes) cannot
 // fire for the reference's pool of 2N + 4096 nodes: a tree has at most N leaves
 // and at most 10 * N / 17 internal nodes. The kernels flag a pool where it could.
+//
+// Every kernel works on a batch of galaxies: a build tile (1024 particles) lies
+// inside one galaxy, each galaxy is numbered in its own node pool exactly as a
+// solo build would number it, and node/particle indices in the arrays are pool
+// indices (the galaxy's node_off / off added).
 #pragma once
 #include "common.cuh"
 #include "morton.cuh"
@@ -39,44 +44,43 @@ __device__ inline int cpd(uint32_t a, uint32_t b) {
 }
 
 struct BuildBuffers {
-  const uint32_t* codes;  // sorted codes [N]
-  uint32_t N;
-  uint32_t cap;           // node pool size
-  uint32_t max_nodes;     // MortonTree pool whose third leaf clause is checked
-  uint8_t* dl;            // packed D | L << 4 per particle [N]
-  uint32_t* blk_counts;   // [blocks][12]
-  uint32_t* blk_offs;     // [blocks][12]
-  TreeMeta* meta;
-  uint32_t* node_start;   // [cap]
-  uint32_t* child_base;   // [cap]
-  int32_t* parent;        // [cap]
-  uint8_t* depth;         // [cap]
-  uint32_t* arrive;       // [cap], zero between builds
-  uint32_t* leaf_node;    // [N + 1]
-  uint32_t* leaf_start;   // [N + 1]
-  float4* cm;             // [cap] com.xyz, mass
-  WalkInfo* info;         // [cap]
+  const uint32_t* codes;  // sorted codes [pool]
+  uint8_t* dl;            // packed D | L << 4 per particle [pool]
+  uint32_t* blk_counts;   // [flag tiles][12]
+  uint32_t* blk_offs;     // [flag tiles][12]
+  TreeMeta* meta;         // [slots]
+  uint32_t* node_start;   // [node pool] first particle of the node
+  uint32_t* child_base;   // [node pool]
+  int32_t* parent;        // [node pool]
+  uint8_t* depth;         // [node pool]
+  uint32_t* arrive;       // [node pool], zero between builds
+  uint32_t* leaf_node;    // [pool] leaf nodes of a galaxy at [off, off + leaves)
+  uint32_t* leaf_start;   // [pool]
+  float4* cm;             // [node pool] com.xyz, mass
+  WalkInfo* info;         // [node pool]
 };
 
-// K1: per particle D, L and per-block start counts.
-__global__ void __launch_bounds__(kFlagThreads) tree_flags_kernel(BuildBuffers b, DevState* st) {
+// K1: per particle D, L and per-tile start counts.
+__global__ void __launch_bounds__(kFlagThreads) tree_flags_kernel(BuildBuffers b, Layout Lo) {
   __shared__ uint32_t s_code[kFlagTile + 32];
   __shared__ int8_t s_cpd16[kFlagTile + 16];
   __shared__ uint32_t s_red[kFlagThreads / 32][kCounters];
   const int tid = threadIdx.x;
-  const int64_t base = (int64_t)blockIdx.x * kFlagTile;
-  const uint32_t N = b.N;
-  if (st && blockIdx.x == 0 && tid < 2) st->central[tid] = st->central_next[tid];
-  // codes [base-16, base+tile+16)
+  const uint32_t tile = blockIdx.x;
+  const SegDesc sd = Lo.segs[Lo.seg_of_flag_tile[tile]];
+  const int64_t seg_beg = sd.off, seg_end = (int64_t)sd.off + sd.n;
+  const int64_t base = seg_beg + (int64_t)(tile - sd.flag_tile0) * kFlagTile;
+  // codes [base-16, base+tile+16) of this galaxy
   for (int k = tid; k < kFlagTile + 32; k += kFlagThreads) {
     const int64_t g = base - 16 + k;
-    s_code[k] = (g >= 0 && g < N) ? b.codes[g] : 0u;
+    s_code[k] = (g >= seg_beg && g < seg_end) ? b.codes[g] : 0u;
   }
   __syncthreads();
-  // cpd16(j) for j in [base-16, base+tile): -1 when j < 0 or j + 16 >= N
+  // cpd16(j) for j in [base-16, base+tile): -1 unless j and j + 16 are in the galaxy
   for (int k = tid; k < kFlagTile + 16; k += kFlagThreads) {
     const int64_t j = base - 16 + k;
-    s_cpd16[k] = (j >= 0 && j + 16 < (int64_t)N) ? (int8_t)cpd(s_code[k], s_code[k + 16]) : (int8_t)-1;
+    s_cpd16[k] = (j >= seg_beg && j + 16 < seg_end) ? (int8_t)cpd(s_code[k], s_code[k + 16])
+                                                    : (int8_t)-1;
   }
   __syncthreads();
   uint32_t cnt[kCounters];
@@ -87,9 +91,9 @@ __global__ void __launch_bounds__(kFlagThreads) tree_flags_kernel(BuildBuffers b
   for (int q = 0; q < kFlagPer; q++) {
     const int loc = tid * kFlagPer + q;
     const int64_t i = base + loc;
-    if (i >= N) break;
+    if (i >= seg_end) break;
     int D;
-    if (i == 0) {
+    if (i == seg_beg) {
       D = 0;
     } else {
       const uint32_t a = s_code[loc + 15], c = s_code[loc + 16];
@@ -105,12 +109,12 @@ __global__ void __launch_bounds__(kFlagThreads) tree_flags_kernel(BuildBuffers b
     cnt[11] += (D <= L) ? 1u : 0u;
   }
   // store packed bytes (4 consecutive particles per thread)
-  if (base + tid * kFlagPer < N) {
-    if (base + tid * kFlagPer + kFlagPer <= N) {
-      reinterpret_cast<uint32_t*>(b.dl)[(base >> 2) + tid] = packed;
+  const int64_t i0 = base + tid * kFlagPer;
+  if (i0 < seg_end) {
+    if (i0 + kFlagPer <= seg_end && (i0 & 3) == 0) {
+      reinterpret_cast<uint32_t*>(b.dl)[i0 >> 2] = packed;
     } else {
-      for (int q = 0; q < kFlagPer && base + tid * kFlagPer + q < N; q++)
-        b.dl[base + tid * kFlagPer + q] = (uint8_t)(packed >> (8 * q));
+      for (int q = 0; q < kFlagPer && i0 + q < seg_end; q++) b.dl[i0 + q] = (uint8_t)(packed >> (8 * q));
     }
   }
   const int warp = tid >> 5, lane = tid & 31;
@@ -123,21 +127,24 @@ __global__ void __launch_bounds__(kFlagThreads) tree_flags_kernel(BuildBuffers b
   if (tid < kCounters) {
     uint32_t s = 0;
     for (int w = 0; w < kFlagThreads / 32; w++) s += s_red[w][tid];
-    b.blk_counts[(size_t)blockIdx.x * kCounters + tid] = s;
+    b.blk_counts[(size_t)tile * kCounters + tid] = s;
   }
 }
 
-// K2: one block scans the per-block counts and fills TreeMeta.
+// K2: one block per galaxy scans its tiles' counts and fills its TreeMeta.
+// root size: the galaxy's Morton frame (frames != NULL) or root_size.
 constexpr int kScanThreads = 1024;
-__global__ void __launch_bounds__(kScanThreads) tree_scan_kernel(BuildBuffers b, uint32_t nblocks,
-                                                                  double root_size,
-                                                                  const MortonFrame* frame,
-                                                                  DevState* st) {
+__global__ void __launch_bounds__(kScanThreads)
+    tree_scan_kernel(BuildBuffers b, Layout Lo, double root_size, const MortonFrame* frames,
+                     DevState* st) {
   __shared__ uint32_t s_warp[kScanThreads / 32][kCounters];
   __shared__ uint32_t s_tot[kCounters];
+  const uint32_t seg = blockIdx.x;
+  const SegDesc sd = Lo.segs[seg];
+  const uint32_t t0 = sd.flag_tile0, ntiles = (sd.n + kFlagTile - 1) / kFlagTile;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t per = (nblocks + kScanThreads - 1) / kScanThreads;
-  const uint32_t b0 = tid * per, b1 = min(nblocks, b0 + per);
+  const uint32_t per = (ntiles + kScanThreads - 1) / kScanThreads;
+  const uint32_t b0 = t0 + min(ntiles, tid * per), b1 = t0 + min(ntiles, tid * per + per);
   uint32_t sum[kCounters];
 #pragma unroll
   for (int k = 0; k < kCounters; k++) sum[k] = 0;
@@ -190,21 +197,25 @@ __global__ void __launch_bounds__(kScanThreads) tree_scan_kernel(BuildBuffers b,
     m.num_nodes = run;
     m.num_levels = levels;
     m.num_leaves = s_tot[11];
-    m.overflow = run > b.cap ? 1u : 0u;
-    m.root_size = frame ? frame->size : root_size;
-    *b.meta = m;
-    if (m.overflow && st) raise_err(st, GS_DERR_NODES);
+    m.overflow = run > sd.node_cap ? 1u : 0u;
+    m.root_size = frames ? frames[sd.slot].size : root_size;
+    b.meta[sd.slot] = m;
+    if (m.overflow) raise_err(st + sd.slot, GS_DERR_NODES);
   }
 }
 
 // K3: node indices, parents, child bases, leaf lists.
-__global__ void __launch_bounds__(kFlagThreads) tree_emit_kernel(BuildBuffers b, DevState* st) {
+__global__ void __launch_bounds__(kFlagThreads) tree_emit_kernel(BuildBuffers b, Layout Lo,
+                                                                  DevState* st) {
   __shared__ uint32_t s_warp[kFlagThreads / 32][kCounters];
   __shared__ TreeMeta s_meta;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int64_t base = (int64_t)blockIdx.x * kFlagTile;
-  const uint32_t N = b.N;
-  if (tid == 0) s_meta = *b.meta;
+  const uint32_t tile = blockIdx.x;
+  const uint32_t seg = Lo.seg_of_flag_tile[tile];
+  const SegDesc sd = Lo.segs[seg];
+  const int64_t seg_end = (int64_t)sd.off + sd.n;
+  const int64_t base = (int64_t)sd.off + (int64_t)(tile - sd.flag_tile0) * kFlagTile;
+  if (tid == 0) s_meta = b.meta[sd.slot];
   uint8_t dl[kFlagPer];
   uint32_t cnt[kCounters];
 #pragma unroll
@@ -212,9 +223,9 @@ __global__ void __launch_bounds__(kFlagThreads) tree_emit_kernel(BuildBuffers b,
 #pragma unroll
   for (int q = 0; q < kFlagPer; q++) {
     const int64_t i = base + tid * kFlagPer + q;
-    dl[q] = i < N ? b.dl[i] : (uint8_t)0;
+    dl[q] = i < seg_end ? b.dl[i] : (uint8_t)0;
     const int D = dl[q] & 15, L = dl[q] >> 4;
-    if (i < N) {
+    if (i < seg_end) {
 #pragma unroll
       for (int d = 0; d < kDepths; d++) cnt[d] += (D <= d && d <= L) ? 1u : 0u;
       cnt[11] += (D <= L) ? 1u : 0u;
@@ -234,7 +245,7 @@ __global__ void __launch_bounds__(kFlagThreads) tree_emit_kernel(BuildBuffers b,
   }
   __syncthreads();
   if (tid < kCounters) {
-    uint32_t run = b.blk_offs[(size_t)blockIdx.x * kCounters + tid];
+    uint32_t run = b.blk_offs[(size_t)tile * kCounters + tid];
     for (int w = 0; w < kFlagThreads / 32; w++) {
       const uint32_t t = s_warp[w][tid];
       s_warp[w][tid] = run;
@@ -246,27 +257,29 @@ __global__ void __launch_bounds__(kFlagThreads) tree_emit_kernel(BuildBuffers b,
 #pragma unroll
   for (int k = 0; k < kCounters; k++) excl[k] += s_warp[warp][k];
   const uint32_t* LS = s_meta.level_start;
+  const uint32_t no = sd.node_off;
 #pragma unroll
   for (int q = 0; q < kFlagPer; q++) {
     const int64_t i = base + tid * kFlagPer + q;
-    if (i >= N) break;
+    if (i >= seg_end) break;
     const int D = dl[q] & 15, L = dl[q] >> 4;
     for (int d = D; d <= L; d++) {
-      const uint32_t n = LS[d] + excl[d];
+      const uint32_t nl = LS[d] + excl[d];  // index within the galaxy's tree
+      const uint32_t n = no + nl;
       b.node_start[n] = (uint32_t)i;
       b.depth[n] = (uint8_t)d;
       // first depth-(d+1) node at or after particle i (children of n start here)
-      b.child_base[n] = d < kMaxLevel ? LS[d + 1] + excl[d + 1] : LS[kDepths];
+      b.child_base[n] = no + (d < kMaxLevel ? LS[d + 1] + excl[d + 1] : LS[kDepths]);
       // parent: the depth-(d-1) node containing i (inclusive count - 1)
       b.parent[n] = d == 0 ? -1
-                           : (int32_t)(LS[d - 1] + excl[d - 1] +
+                           : (int32_t)(no + LS[d - 1] + excl[d - 1] +
                                        ((D <= d - 1 && d - 1 <= L) ? 1u : 0u) - 1u);
       if (d == L) {
-        b.leaf_node[excl[11]] = n;
-        b.leaf_start[excl[11]] = (uint32_t)i;
+        b.leaf_node[sd.off + excl[11]] = n;
+        b.leaf_start[sd.off + excl[11]] = (uint32_t)i;
       }
       // mortonTree.js:127: an internal node with numNodes + 8 > maxNodes would be a leaf
-      if (d < L && n + 1 + 8 > b.max_nodes && st) raise_err(st, GS_DERR_NODES);
+      if (d < L && nl + 1 + 8 > sd.max_nodes) raise_err(st + sd.slot, GS_DERR_NODES);
     }
 #pragma unroll
     for (int d = 0; d < kDepths; d++) excl[d] += (D <= d && d <= L) ? 1u : 0u;
@@ -274,12 +287,15 @@ __global__ void __launch_bounds__(kFlagThreads) tree_emit_kernel(BuildBuffers b,
   }
 }
 
-__device__ inline uint32_t child_count(const BuildBuffers& b, const TreeMeta& m, uint32_t p) {
+// Children of internal node p (pool index) of a galaxy: [child_base[p], + count).
+__device__ inline uint32_t child_count(const BuildBuffers& b, const TreeMeta& m, uint32_t node_off,
+                                       uint32_t p) {
   const int d = b.depth[p];
   const uint32_t cb = b.child_base[p];
+  const uint32_t pl = p - node_off;
   const uint32_t level_end = m.level_start[d] + m.level_count[d];
-  const uint32_t next = (p + 1 < level_end) ? __ldcg(&b.child_base[p + 1])
-                                            : m.level_start[d + 1] + m.level_count[d + 1];
+  const uint32_t next = (pl + 1 < level_end) ? __ldcg(&b.child_base[p + 1])
+                                             : node_off + m.level_start[d + 1] + m.level_count[d + 1];
   return next - cb;
 }
 
@@ -290,23 +306,30 @@ enum ComMode : int {
   kComF64 = 2,   // FP32 leaves, FP64 internal nodes (large-node reduction in double)
 };
 
-// K4: one thread per leaf; leaf COM, then carry each finished node to its
-// parent; the last child to finish sums the parent (children in slot order).
+// K4: one thread per leaf slot (a block per build tile, kLeafThreads = one
+// tile); leaf COM, then carry each finished node to its parent; the last child
+// to finish sums the parent (children in slot order).
+constexpr int kLeafThreads = kFlagTile;
 template <int MODE>
-__global__ void __launch_bounds__(256) tree_leaves_kernel(BuildBuffers b, const float4* __restrict__ pos,
-                                                          uint32_t pos_stride, DevState* st) {
-  __shared__ TreeMeta s_meta;
-  if (threadIdx.x == 0) s_meta = *b.meta;
-  __syncthreads();
-  const TreeMeta& m = s_meta;
-  if (m.overflow) return;
-  const uint32_t nleaves = m.num_leaves;
-  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nleaves; r += gridDim.x * blockDim.x) {
+__global__ void __launch_bounds__(kLeafThreads)
+    tree_leaves_kernel(BuildBuffers b, Layout Lo, const float4* __restrict__ pos,
+                       uint32_t pos_stride, DevState* st) {
+  do {  // `continue` leaves the block's single iteration
+    const uint32_t tile = blockIdx.x;
+    const SegDesc sd = Lo.segs[Lo.seg_of_flag_tile[tile]];
+    const uint32_t lr = (tile - sd.flag_tile0) * kFlagTile + threadIdx.x;  // leaf slot in the galaxy
+    const uint32_t r = sd.off + lr;
+    const TreeMeta& m = b.meta[sd.slot];
+    if (m.overflow) continue;
+    const uint32_t nleaves = m.num_leaves;
+    if (lr >= nleaves) continue;
+    const uint32_t seg_end = sd.off + sd.n;
+    const uint32_t node_end = sd.node_off + m.num_nodes;
     uint32_t n = b.leaf_node[r];
     const uint32_t lo = b.leaf_start[r];
-    const uint32_t hi = (r + 1 < nleaves) ? b.leaf_start[r + 1] : b.N;
-    if (n >= m.num_nodes || hi < lo || hi > b.N) {  // impossible for a correct emit
-      if (st) raise_err(st, GS_DERR_NODES);
+    const uint32_t hi = (lr + 1 < nleaves) ? b.leaf_start[r + 1] : seg_end;
+    if (n < sd.node_off || n >= node_end || hi < lo || lo < sd.off || hi > seg_end) {
+      raise_err(st + sd.slot, GS_DERR_NODES);  // impossible for a correct emit
       continue;
     }
     const int d = b.depth[n];
@@ -347,10 +370,11 @@ __global__ void __launch_bounds__(256) tree_leaves_kernel(BuildBuffers b, const 
     while (true) {
       const int32_t p = b.parent[n];
       if (p < 0) break;
-      const uint32_t nc = (uint32_t)p < n ? child_count(b, m, (uint32_t)p) : 0u;
-      if ((uint32_t)p >= n || nc == 0 || nc > 8 ||
-          (uint64_t)b.child_base[p] + nc > m.num_nodes) {  // parents precede children in BFS
-        if (st) raise_err(st, GS_DERR_NODES);
+      const uint32_t nc =
+          ((uint32_t)p < n && (uint32_t)p >= sd.node_off) ? child_count(b, m, sd.node_off, (uint32_t)p) : 0u;
+      if ((uint32_t)p >= n || (uint32_t)p < sd.node_off || nc == 0 || nc > 8 ||
+          (uint64_t)b.child_base[p] + nc > node_end) {  // parents precede children in BFS
+        raise_err(st + sd.slot, GS_DERR_NODES);
         break;
       }
       // release: this node's COM is visible before the count; acquire: the last
@@ -403,13 +427,16 @@ __global__ void __launch_bounds__(256) tree_leaves_kernel(BuildBuffers b, const 
       b.info[p] = pw;
       n = (uint32_t)p;
     }
-  }
+  } while (0);
 }
 
-// BHNode materialisation (API only): the 64-byte layout of mortonTree.js:12-20.
-__global__ void tree_bhnode_kernel(BuildBuffers b, gs_node* out) {
-  const TreeMeta m = *b.meta;
-  for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < m.num_nodes; n += gridDim.x * blockDim.x) {
+// BHNode materialisation of one galaxy (API only): the 64-byte layout of
+// mortonTree.js:12-20 with indices local to the galaxy, as a solo build has them.
+__global__ void tree_bhnode_kernel(BuildBuffers b, Layout Lo, uint32_t seg, gs_node* out) {
+  const SegDesc sd = Lo.segs[seg];
+  const TreeMeta m = b.meta[sd.slot];
+  for (uint32_t nl = blockIdx.x * blockDim.x + threadIdx.x; nl < m.num_nodes; nl += gridDim.x * blockDim.x) {
+    const uint32_t n = sd.node_off + nl;
     const float4 c = b.cm[n];
     const WalkInfo w = b.info[n];
     gs_node o;
@@ -421,7 +448,7 @@ __global__ void tree_bhnode_kernel(BuildBuffers b, gs_node* out) {
     for (int k = 0; k < 8; k++) o.children[k] = -1;
     if (w.info & kLeafBit) {
       o.isLeaf = 1;
-      o.first = w.child;
+      o.first = w.child - sd.off;
       o.count = w.info & ~kLeafBit;
     } else {
       o.isLeaf = 0;
@@ -430,14 +457,14 @@ __global__ void tree_bhnode_kernel(BuildBuffers b, gs_node* out) {
       const int shift = 27 - 3 * min((int)b.depth[n], 9);
       for (uint32_t k = 0; k < w.info && k < 8; k++) {
         const uint32_t ch = w.child + k;
-        if (ch >= m.num_nodes) break;
+        if (ch < sd.node_off || ch >= sd.node_off + m.num_nodes) break;
         const uint32_t ps = b.node_start[ch];
-        if (ps >= b.N) break;
+        if (ps < sd.off || ps >= sd.off + sd.n) break;
         const uint32_t oct = (b.codes[ps] >> shift) & 7u;
-        o.children[oct] = (int32_t)ch;
+        o.children[oct] = (int32_t)(ch - sd.node_off);
       }
     }
-    out[n] = o;
+    out[nl] = o;
   }
 }
 

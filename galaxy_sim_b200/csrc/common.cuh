@@ -23,19 +23,18 @@ struct __align__(16) WalkInfo {
 };
 constexpr uint32_t kLeafBit = 0x80000000u;
 
-// Device copy of the per-step physics state (Params + what main.js keeps).
+// Per-galaxy copy of the physics state (Params + what main.js keeps).
 struct __align__(16) DevState {
   gs_params p;            // 96 B Params, time refreshed from sim_time each step
   double sim_time;        // main.js simTime (JS number)
   double halo_c[2][3];    // smoothed halo centres (main.js haloCenters, doubles)
-  long long central[2];   // tracked central particle indices, -1 = none
-  long long central_next[2];  // written by the gather, published by the next kernel
+  long long central[2];   // tracked central particles (particle-pool indices), -1 = none
   unsigned int err;       // GS_DERR_* bits
   unsigned int pad_;
   unsigned long long counters[3];  // monopoles, leaf pairs, node visits
 };
 
-// Tree build scalar outputs.
+// Tree build scalar outputs of one galaxy (node indices local to its pool).
 struct __align__(16) TreeMeta {
   uint32_t level_start[kDepths + 1];
   uint32_t level_count[kDepths + 1];
@@ -46,11 +45,30 @@ struct __align__(16) TreeMeta {
   double root_size;
 };
 
-// Morton bounding box: ordered-int encodings of float min/max (atomics).
-struct __align__(16) BBox {
-  int mn[3];
-  int mx[3];
-  int pad_[2];
+// One galaxy ("segment") of a batch: a contiguous particle range with its own
+// node pool, Morton frame, tree and Params. A single simulation is a batch of one.
+struct __align__(16) SegDesc {
+  uint32_t off, n;              // particles [off, off + n) of the particle pool
+  uint32_t node_off, node_cap;  // nodes [node_off, node_off + node_cap) of the node pool
+  uint32_t sort_tile0;          // first sort tile of the batch's tile list
+  uint32_t flag_tile0;          // first build tile (also bbox, codes, gather tiles)
+  uint32_t group0;              // first walk group
+  uint32_t max_nodes;           // pool of MortonTree's third leaf clause (2n + 4096)
+  uint32_t slot;                // index of the galaxy's DevState, TreeMeta, frame, histograms
+  uint32_t diag_chunk0;         // first block of the diagnostics reduction
+  uint32_t pad_[2];
+};
+
+// Device view of a batch's layout: segments (sorted by particle offset) and the
+// maps from each tile / walk group to its segment. Tiles never cross segments;
+// the pool between segments holds free holes that no tile covers.
+struct Layout {
+  const SegDesc* segs;
+  const uint32_t* seg_of_sort_tile;
+  const uint32_t* seg_of_flag_tile;
+  const uint32_t* seg_of_group;
+  uint32_t nseg;
+  uint32_t sort_tiles, flag_tiles, groups, diag_chunks;
 };
 
 __device__ inline int float_to_ordered(float f) {

@@ -1,9 +1,21 @@
 // Host runtime and C ABI of the B200 gravity path (declarations and reference
-// citations in include/galaxy_b200.h). One gs_ctx owns its device memory and
-// one CUDA stream; every operation is stream-ordered like the WebGPU command
-// encoder it replaces, and full steps are replayed from captured CUDA graphs.
+// citations in include/galaxy_b200.h).
+//
+// A context is a pool of galaxy slots over one set of device buffers and one
+// CUDA stream. Every operation is stream-ordered like the WebGPU command encoder
+// it replaces; full steps of all resident galaxies are one launch per kernel
+// (segmented sort, build and walk), replayed from captured CUDA graphs.
+//
+// Pool memory: particle records live at [off, off + n) of the particle pool
+// (offsets aligned to kAlign), the galaxy's nodes at [2 off, 2 off + 2 n) of
+// the node pool. A bucketed octree of n particles has at most n leaves (every
+// leaf holds a particle) and at most n / 17 internal nodes per depth 0..9, so
+// at most 1.59 n nodes: node ranges never overlap and need no allocator of
+// their own. A single-galaxy context gives its galaxy 2 n + 4096 nodes, the
+// reference's MortonTree pool, so any uploaded tree of that size fits.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -27,21 +39,140 @@ namespace {
 
 thread_local char g_err[512] = "";
 
-constexpr uint32_t kMaxN = 1u << 27;  // node indices (2N + 4096) fit the walk's 29-bit fields
-constexpr int kSortPasses = 4;
+constexpr uint64_t kMaxPool = 1ull << 27;  // node indices (2 cap + 4096) fit the walk's 29-bit fields
+constexpr uint32_t kMaxSlots = 4096;
+constexpr uint32_t kAlign = 256;           // particle offset alignment of a galaxy
 
 inline uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
 
-// Device workspace of one sort + build over up to N particles.
-struct Workspace {
-  uint32_t N = 0, cap = 0, tiles = 0, fblocks = 0;
+void set_err(char* dst, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(dst, 512, fmt, ap);
+  va_end(ap);
+}
+
+uint32_t grid_for(uint64_t N, uint32_t threads, uint32_t cap_blocks) {
+  return std::min<uint32_t>(cap_blocks, std::max<uint32_t>(1, cdiv(N, threads)));
+}
+
+// Sizes of every pool buffer for a particle capacity and slot count.
+struct Plan {
+  uint64_t cap = 0, nodes = 0;
+  uint32_t slots = 0, sort_tiles = 0, flag_tiles = 0, groups = 0, diag_chunks = 0;
+  size_t sort_words = 0;  // hist[slots][4][256] | tile counters[16] | look-back[4][tiles][256]
+};
+
+Plan make_plan(uint64_t cap, uint32_t slots) {
+  Plan p;
+  p.cap = cap;
+  p.slots = slots;
+  p.nodes = 2 * cap + 4096;
+  p.sort_tiles = cdiv(cap, kSortTile) + slots;
+  p.flag_tiles = cdiv(cap, kFlagTile) + slots;
+  p.groups = cdiv(cap, kWalkGroup) + slots;
+  p.diag_chunks = cdiv(p.groups, kDiagChunk) + slots;
+  p.sort_words = (size_t)slots * kSortPasses * 256 + 16 + (size_t)kSortPasses * p.sort_tiles * 256;
+  return p;
+}
+
+// Device bytes a pool allocates (the debug force buffers and the BHNode staging
+// of gs_get_tree / gs_upload_tree come on demand and are not included).
+uint64_t plan_bytes(const Plan& p) {
+  const uint64_t c = p.cap, n = p.nodes, s = p.slots;
+  uint64_t b = 0;
+  b += c * (2 * 32 + 2 * 16 + 4 + 16 + 4 + 4);   // particles x2, stellar x2, energy, compact, perm, inv
+  b += c * (4 * 4 + 1 + 2 * 4) + 2 * 4 + 4;     // keys x2, vals x2, dl, leaf lists
+  b += p.sort_words * 4;
+  b += (uint64_t)p.flag_tiles * (6 * 4 + 2 * kCounters * 4);
+  b += n * (16 + 16 + 4 + 4 + 4 + 1 + 4) + 4;   // cm, info, node_start, child_base, parent, depth, arrive
+  b += s * (sizeof(DevState) + sizeof(TreeMeta) + sizeof(MortonFrame) + 4 + kPartials * 8 + sizeof(SegDesc));
+  b += (uint64_t)(p.sort_tiles + p.flag_tiles + p.groups) * 4;
+  b += (uint64_t)p.groups * kPartials * 8 + 16;
+  b += (uint64_t)p.diag_chunks * kPartials * 8 + s * 4;
+  return b;
+}
+
+// First-fit allocator of particle ranges (free holes keyed by offset).
+struct RangeAlloc {
+  std::map<uint64_t, uint64_t> free;  // off -> len
+  void init(uint64_t cap) {
+    free.clear();
+    if (cap) free[0] = cap;
+  }
+  bool alloc(uint64_t len, uint64_t* off) {
+    for (auto it = free.begin(); it != free.end(); ++it) {
+      if (it->second < len) continue;
+      *off = it->first;
+      const uint64_t rest = it->second - len;
+      free.erase(it);
+      if (rest) free[*off + len] = rest;
+      return true;
+    }
+    return false;
+  }
+  void release(uint64_t off, uint64_t len) {
+    auto it = free.emplace(off, len).first;
+    auto nx = std::next(it);
+    if (nx != free.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free.erase(nx);
+    }
+    if (it != free.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free.erase(it);
+      }
+    }
+  }
+  uint64_t largest() const {
+    uint64_t m = 0;
+    for (auto& kv : free) m = std::max(m, kv.second);
+    return m;
+  }
+};
+
+struct Slot {
+  bool live = false;
+  uint32_t off = 0, n = 0, span = 0;  // span: the allocated (aligned) particle range
+  uint32_t node_off = 0, node_cap = 0;
+  gs_params hp{};
+  bool tracking = false;
+  enum { kTreeNone, kTreeUploaded, kTreeBuilt } tree = kTreeNone;
+  uint32_t up_nodes = 0;
+  std::vector<uint32_t> up_lr;
+  std::vector<gs_node> up_host;  // the uploaded BHNodes (COM patched on readback)
+  uint32_t max_nodes = 0;        // MortonTree pool of the leaf clause (0: 2n + 4096)
+  uint32_t rank = 0;             // position in the current layout
+};
+
+}  // namespace
+
+struct gs_ctx {
+  int device = 0;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev = nullptr;
+  Plan plan;
+  std::vector<void*> owned;
+  // particle pool
+  float4* part[2] = {nullptr, nullptr};
+  float4* stel[2] = {nullptr, nullptr};
+  int cur = 0, scur = 0;
+  float* energy = nullptr;
+  float4* compact = nullptr;
+  uint32_t* perm_user = nullptr;
+  uint32_t* inv = nullptr;
+  // sort
   uint32_t* keys[2] = {nullptr, nullptr};
   uint32_t* vals[2] = {nullptr, nullptr};
-  uint32_t* sort_scratch = nullptr;  // hist[4*256] | tile counters[16] | lookback
-  size_t sort_scratch_bytes = 0;
-  int* bbox_partials = nullptr;
-  unsigned* bbox_counter = nullptr;
-  MortonFrame* frame = nullptr;
+  uint32_t* sort_scratch = nullptr;
+  // bbox / frames
+  int* bbox_part = nullptr;
+  unsigned* seg_ctr = nullptr;
+  MortonFrame* frames = nullptr;
+  // build
   uint8_t* dl = nullptr;
   uint32_t* blk_counts = nullptr;
   uint32_t* blk_offs = nullptr;
@@ -55,192 +186,38 @@ struct Workspace {
   uint32_t* leaf_start = nullptr;
   float4* cm = nullptr;
   WalkInfo* info = nullptr;
-  std::vector<void*> owned;
-
-  uint32_t* hist() const { return sort_scratch; }
-  uint32_t* tile_ctr() const { return sort_scratch + 4 * 256; }
-  uint32_t* lookback() const { return sort_scratch + 4 * 256 + 16; }
-
-  BuildBuffers bb(uint32_t max_nodes) const {
-    BuildBuffers b;
-    b.codes = keys[0];
-    b.N = N;
-    b.cap = cap;
-    b.max_nodes = max_nodes;
-    b.dl = dl;
-    b.blk_counts = blk_counts;
-    b.blk_offs = blk_offs;
-    b.meta = meta;
-    b.node_start = node_start;
-    b.child_base = child_base;
-    b.parent = parent;
-    b.depth = depth;
-    b.arrive = arrive;
-    b.leaf_node = leaf_node;
-    b.leaf_start = leaf_start;
-    b.cm = cm;
-    b.info = info;
-    return b;
-  }
-
-  template <typename T>
-  cudaError_t alloc(T** p, size_t count) {
-    void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, count * sizeof(T) + 16);
-    if (e != cudaSuccess) return e;
-    owned.push_back(q);
-    *p = reinterpret_cast<T*>(q);
-    return cudaSuccess;
-  }
-  cudaError_t init(uint32_t n) {
-    N = n;
-    cap = 2 * n + 4096;
-    tiles = cdiv(n, kSortTile);
-    fblocks = cdiv(n, kFlagTile);
-    cudaError_t e;
-#define A(ptr, cnt)                  \
-  if ((e = alloc(&(ptr), (cnt))) != cudaSuccess) return e;
-    A(keys[0], n);
-    A(keys[1], n);
-    A(vals[0], n);
-    A(vals[1], n);
-    sort_scratch_bytes = sizeof(uint32_t) * (4 * 256 + 16 + (size_t)kSortPasses * tiles * 256);
-    A(sort_scratch, sort_scratch_bytes / sizeof(uint32_t));
-    A(bbox_partials, kBBoxBlocks * 6);
-    A(bbox_counter, 4);
-    A(frame, 1);
-    A(dl, n + 4);
-    A(blk_counts, (size_t)fblocks * kCounters);
-    A(blk_offs, (size_t)fblocks * kCounters);
-    A(meta, 1);
-    A(node_start, cap);
-    A(child_base, cap + 1);
-    A(parent, cap);
-    A(depth, cap);
-    A(arrive, cap);
-    A(leaf_node, n + 1);
-    A(leaf_start, n + 1);
-    A(cm, cap);
-    A(info, cap);
-#undef A
-    if ((e = cudaMemset(bbox_counter, 0, 16)) != cudaSuccess) return e;
-    if ((e = cudaMemset(arrive, 0, sizeof(uint32_t) * cap)) != cudaSuccess) return e;
-    if ((e = cudaMemset(cm, 0, sizeof(float4) * cap)) != cudaSuccess) return e;
-    if ((e = cudaMemset(info, 0, sizeof(WalkInfo) * cap)) != cudaSuccess) return e;
-    return cudaSuccess;
-  }
-  void release() {
-    for (void* p : owned) cudaFree(p);
-    owned.clear();
-  }
-};
-
-// codes of `pos` (float4 records, stride in float4) into keys[0], sort -> keys[0]
-// (sorted codes) and vals[0] (gather permutation).
-cudaError_t enqueue_codes_sort(Workspace& w, const float4* pos, uint32_t stride, cudaStream_t s,
-                               DevState* st, int advance_time) {
-  const uint32_t N = w.N;
-  const uint32_t bb = std::min<uint32_t>(kBBoxBlocks, std::max<uint32_t>(1, cdiv(N, kBBoxThreads)));
-  bbox_kernel<<<bb, kBBoxThreads, 0, s>>>(pos, stride, N, w.bbox_partials, w.bbox_counter, w.frame,
-                                          st, advance_time);
-  cudaMemsetAsync(w.sort_scratch, 0, w.sort_scratch_bytes, s);
-  const uint32_t cb = std::min<uint32_t>(148 * 8, std::max<uint32_t>(1, cdiv(N, 256)));
-  codes_kernel<<<cb, 256, 0, s>>>(pos, stride, N, w.frame, w.keys[0], w.hist(), kSortPasses);
-  for (int p = 0; p < kSortPasses; p++) {
-    const int src = p & 1, dst = src ^ 1;
-    uint32_t* lb = w.lookback() + (size_t)p * w.tiles * 256;
-    if (p == 0)
-      onesweep_pass<true><<<w.tiles, kSortThreads, 0, s>>>(w.keys[src], nullptr, w.keys[dst],
-                                                           w.vals[dst], w.hist() + p * 256, lb,
-                                                           w.tile_ctr() + p, N, 8 * p, st);
-    else
-      onesweep_pass<false><<<w.tiles, kSortThreads, 0, s>>>(w.keys[src], w.vals[src], w.keys[dst],
-                                                            w.vals[dst], w.hist() + p * 256, lb,
-                                                            w.tile_ctr() + p, N, 8 * p, st);
-  }
-  return cudaGetLastError();
-}
-
-// hist of given keys (stateless radix sort)
-__global__ void key_hist_kernel(const uint32_t* __restrict__ keys, uint32_t N, uint32_t* hist,
-                                int passes) {
-  __shared__ uint32_t s_hist[4 * 256];
-  for (int k = threadIdx.x; k < 4 * 256; k += blockDim.x) s_hist[k] = 0;
-  __syncthreads();
-  for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < N; i0 += gridDim.x * blockDim.x) {
-    const uint32_t i = i0 + threadIdx.x;
-    const bool valid = i < N;
-    hist_add_warp(s_hist, valid ? keys[i] : 0u, valid, passes);
-  }
-  __syncthreads();
-  for (int k = threadIdx.x; k < passes * 256; k += blockDim.x)
-    if (s_hist[k]) atomicAdd(&hist[k], s_hist[k]);
-}
-
-__global__ void mask30_kernel(uint32_t* keys, uint32_t N) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
-    keys[i] &= 0x3fffffffu;
-}
-
-// the tree over keys[0] (sorted codes) with COM from pos
-// root size: the Morton frame of the preceding sort (frame != NULL) or root_size_host.
-cudaError_t enqueue_build(Workspace& w, const float4* pos, uint32_t stride, uint32_t max_nodes,
-                          int com_mode, double root_size_host, const MortonFrame* frame,
-                          cudaStream_t s, DevState* st, DevState* st_flags) {
-  BuildBuffers b = w.bb(max_nodes);
-  tree_flags_kernel<<<w.fblocks, kFlagThreads, 0, s>>>(b, st_flags);
-  tree_scan_kernel<<<1, kScanThreads, 0, s>>>(b, w.fblocks, root_size_host, frame, st);
-  tree_emit_kernel<<<w.fblocks, kFlagThreads, 0, s>>>(b, st);
-  const uint32_t lb = std::min<uint32_t>(148 * 16, std::max<uint32_t>(1, cdiv(w.N, 256)));
-  if (com_mode == kComJs)
-    tree_leaves_kernel<kComJs><<<lb, 256, 0, s>>>(b, pos, stride, st);
-  else if (com_mode == kComF64)
-    tree_leaves_kernel<kComF64><<<lb, 256, 0, s>>>(b, pos, stride, st);
-  else
-    tree_leaves_kernel<kComF32><<<lb, 256, 0, s>>>(b, pos, stride, st);
-  return cudaGetLastError();
-}
-
-void set_err(char* dst, const char* fmt, ...) {
-  va_list ap;
-  va_start(ap, fmt);
-  vsnprintf(dst, 512, fmt, ap);
-  va_end(ap);
-}
-
-}  // namespace
-
-struct gs_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  uint32_t N = 0;
-  Workspace ws;
-  float4* part[2] = {nullptr, nullptr};
-  float4* stel[2] = {nullptr, nullptr};
-  int cur = 0, scur = 0;
-  float* energy = nullptr;
-  float4* compact = nullptr;
-  uint32_t* perm_user = nullptr;
+  // per slot
   DevState* st = nullptr;
-  gs_params hp{};
+  double* diag_out = nullptr;  // [slots][kPartials]
+  double* diag_chunk = nullptr;  // [diag chunks][kPartials]
+  unsigned* diag_ctr = nullptr;  // [slots]
+  // layout
+  SegDesc* segs = nullptr;
+  uint32_t* sort_map = nullptr;
+  uint32_t* flag_map = nullptr;
+  uint32_t* group_map = nullptr;
+  Layout lay{};
+  std::vector<SegDesc> seg_host;  // the layout's galaxies, host copy
+  bool lay_dirty = true;
+  uint32_t hist_slots = 0;  // histogram slots cleared per step (max live slot + 1)
+  // walk
   double* partials = nullptr;
-  double* diag_out = nullptr;
-  uint32_t walk_groups = 0;  // 32-particle groups (diagnostic partials)
-  uint32_t walk_grid = 0;    // persistent walk blocks
   unsigned* walk_work = nullptr;
+  uint32_t walk_grid = 0;
   float4* dbg_acc = nullptr;
   float* dbg_dens = nullptr;
   bool debug = false;
   gs_node* bh = nullptr;  // BHNode staging (upload / materialise)
   uint32_t max_bh = 0;
-  enum { kTreeNone, kTreeUploaded, kTreeBuilt } tree = kTreeNone;
-  uint32_t up_nodes = 0;
-  std::vector<uint32_t> up_lr;
-  bool tracking = false;
+  // slots
+  std::vector<Slot> slots;
+  RangeAlloc palloc;
+  uint32_t sel = 0;
+  bool single = false;  // created by gs_create: one galaxy, node pool 2N + 4096
   int com_mode = kComF32;
-  void* host_stage = nullptr;  // pinned, N * 16 bytes
-  cudaEvent_t ev = nullptr;
+  void* host_stage = nullptr;  // pinned: [slots] params
   std::map<int, cudaGraphExec_t> graphs;
+  uint32_t step_kernels = 0;  // kernel nodes of the last captured step graph
   char err[512] = "";
 
   int fail(int code, const char* fmt, ...) {
@@ -259,6 +236,42 @@ struct gs_ctx {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     graphs.clear();
   }
+  template <typename T>
+  cudaError_t alloc(T** p, size_t count) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T) + 16);
+    if (e != cudaSuccess) return e;
+    owned.push_back(q);
+    *p = reinterpret_cast<T*>(q);
+    return cudaSuccess;
+  }
+  uint32_t* hist() const { return sort_scratch; }
+  uint32_t* tile_ctr() const { return sort_scratch + (size_t)plan.slots * kSortPasses * 256; }
+  uint32_t* lookback() const { return tile_ctr() + 16; }
+  BuildBuffers bb() const {
+    BuildBuffers b;
+    b.codes = keys[0];
+    b.dl = dl;
+    b.blk_counts = blk_counts;
+    b.blk_offs = blk_offs;
+    b.meta = meta;
+    b.node_start = node_start;
+    b.child_base = child_base;
+    b.parent = parent;
+    b.depth = depth;
+    b.arrive = arrive;
+    b.leaf_node = leaf_node;
+    b.leaf_start = leaf_start;
+    b.cm = cm;
+    b.info = info;
+    return b;
+  }
+  bool any_tracking() const {
+    for (const Slot& s : slots)
+      if (s.live && s.tracking) return true;
+    return false;
+  }
+  Slot* selected() { return sel < slots.size() && slots[sel].live ? &slots[sel] : nullptr; }
 };
 
 #define CK(ctx, expr, what)                                    \
@@ -276,39 +289,207 @@ struct gs_ctx {
     cudaSetDevice((ctx)->device);                              \
   } while (0)
 
+// The selected galaxy, or fail with GS_ENOTREADY.
+#define SLOT(ctx, s)                                                                       \
+  Slot* s = (ctx)->selected();                                                             \
+  if (!s) return (ctx)->fail(GS_ENOTREADY, "no galaxy in selected slot %u", (ctx)->sel);
+
 namespace {
 
-uint32_t grid_for(uint32_t N, uint32_t threads, uint32_t cap_blocks) {
-  return std::min<uint32_t>(cap_blocks, std::max<uint32_t>(1, cdiv(N, threads)));
+int pool_init(gs_ctx* c, int device, uint64_t cap, uint32_t slots) {
+  c->device = device;
+  c->plan = make_plan(cap, slots);
+  const Plan& p = c->plan;
+  cudaSetDevice(device);
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+  CK(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
+  CK(c, cudaEventCreateWithFlags(&c->ev, cudaEventDisableTiming), "event");
+#define A(ptr, cnt) CK(c, c->alloc(&(ptr), (cnt)), #ptr)
+  A(c->part[0], 2 * p.cap);
+  A(c->part[1], 2 * p.cap);
+  A(c->stel[0], p.cap);
+  A(c->stel[1], p.cap);
+  A(c->energy, p.cap);
+  A(c->compact, p.cap);
+  A(c->perm_user, p.cap);
+  A(c->inv, p.cap);
+  A(c->keys[0], p.cap);
+  A(c->keys[1], p.cap);
+  A(c->vals[0], p.cap);
+  A(c->vals[1], p.cap);
+  A(c->sort_scratch, p.sort_words);
+  A(c->bbox_part, (size_t)p.flag_tiles * 6);
+  A(c->seg_ctr, p.slots);
+  A(c->frames, p.slots);
+  A(c->dl, p.cap + 4);
+  A(c->blk_counts, (size_t)p.flag_tiles * kCounters);
+  A(c->blk_offs, (size_t)p.flag_tiles * kCounters);
+  A(c->meta, p.slots);
+  A(c->node_start, p.nodes);
+  A(c->child_base, p.nodes + 1);
+  A(c->parent, p.nodes);
+  A(c->depth, p.nodes);
+  A(c->arrive, p.nodes);
+  A(c->leaf_node, p.cap + 1);
+  A(c->leaf_start, p.cap + 1);
+  A(c->cm, p.nodes);
+  A(c->info, p.nodes);
+  A(c->st, p.slots);
+  A(c->diag_out, (size_t)p.slots * kPartials);
+  A(c->diag_chunk, (size_t)p.diag_chunks * kPartials);
+  A(c->diag_ctr, p.slots);
+  A(c->segs, p.slots);
+  A(c->sort_map, p.sort_tiles);
+  A(c->flag_map, p.flag_tiles);
+  A(c->group_map, p.groups);
+  A(c->partials, (size_t)p.groups * kPartials);
+  A(c->walk_work, 4);
+#undef A
+  CK(c, cudaMemset(c->seg_ctr, 0, sizeof(unsigned) * p.slots), "memset");
+  CK(c, cudaMemset(c->arrive, 0, sizeof(uint32_t) * p.nodes), "memset");
+  CK(c, cudaMemset(c->cm, 0, sizeof(float4) * p.nodes), "memset");
+  CK(c, cudaMemset(c->info, 0, sizeof(WalkInfo) * p.nodes), "memset");
+  CK(c, cudaMemset(c->meta, 0, sizeof(TreeMeta) * p.slots), "memset");
+  CK(c, cudaMemset(c->st, 0, sizeof(DevState) * p.slots), "memset");
+  CK(c, cudaMemset(c->diag_out, 0, sizeof(double) * kPartials * p.slots), "memset");
+  CK(c, cudaMemset(c->diag_ctr, 0, sizeof(unsigned) * p.slots), "memset");
+  CK(c, cudaMemset(c->partials, 0, sizeof(double) * kPartials * p.groups), "memset");
+  CK(c, cudaMemset(c->walk_work, 0, 16), "memset");
+  CK(c, cudaMallocHost(&c->host_stage, sizeof(gs_params) * (size_t)p.slots + 256), "pinned stage");
+  c->slots.assign(p.slots, Slot());
+  c->palloc.init(p.cap);
+  c->lay_dirty = true;
+  return GS_OK;
 }
 
-int wait_stream(gs_ctx* c, uint64_t timeout_ns) {
-  CK(c, cudaEventRecord(c->ev, c->stream), "cudaEventRecord");
-  if (timeout_ns == 0) {
-    CK(c, cudaEventSynchronize(c->ev), "cudaEventSynchronize");
-  } else {
-    const auto t0 = std::chrono::steady_clock::now();
-    while (true) {
-      cudaError_t q = cudaEventQuery(c->ev);
-      if (q == cudaSuccess) break;
-      if (q != cudaErrorNotReady) return c->cuda(q, "cudaEventQuery");
-      const auto dt = std::chrono::duration_cast<std::chrono::nanoseconds>(
-                          std::chrono::steady_clock::now() - t0)
-                          .count();
-      if ((uint64_t)dt > timeout_ns)
-        return c->fail(GS_ETIMEDOUT, "stream did not drain within %llu ns",
-                       (unsigned long long)timeout_ns);
-      std::this_thread::sleep_for(std::chrono::microseconds(50));
-    }
+void pool_release(gs_ctx* c) {
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->drop_graphs();
+  for (void* q : c->owned) cudaFree(q);
+  c->owned.clear();
+  if (c->host_stage) cudaFreeHost(c->host_stage);
+  if (c->ev) cudaEventDestroy(c->ev);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  c->host_stage = nullptr;
+  c->ev = nullptr;
+  c->stream = nullptr;
+}
+
+// Rebuild the device layout (galaxies in offset order, tile/group maps) after
+// slots were added or removed. The stream must be idle (no step in flight).
+int ensure_layout(gs_ctx* c) {
+  if (!c->lay_dirty) return GS_OK;
+  std::vector<uint32_t> order;
+  for (uint32_t s = 0; s < c->slots.size(); s++)
+    if (c->slots[s].live) order.push_back(s);
+  std::sort(order.begin(), order.end(),
+            [&](uint32_t a, uint32_t b) { return c->slots[a].off < c->slots[b].off; });
+  std::vector<SegDesc> h(order.size());
+  uint32_t st = 0, ft = 0, gr = 0, dc = 0, hs = 0;
+  for (size_t r = 0; r < order.size(); r++) {
+    Slot& s = c->slots[order[r]];
+    s.rank = (uint32_t)r;
+    SegDesc d;
+    memset(&d, 0, sizeof(d));
+    d.off = s.off;
+    d.n = s.n;
+    d.node_off = s.node_off;
+    d.node_cap = s.node_cap;
+    d.sort_tile0 = st;
+    d.flag_tile0 = ft;
+    d.group0 = gr;
+    d.max_nodes = s.max_nodes ? s.max_nodes : 2 * s.n + 4096;
+    d.slot = order[r];
+    d.diag_chunk0 = dc;
+    h[r] = d;
+    dc += cdiv(cdiv(s.n, kWalkGroup), kDiagChunk);
+    st += cdiv(s.n, kSortTile);
+    ft += cdiv(s.n, kFlagTile);
+    gr += cdiv(s.n, kWalkGroup);
+    hs = std::max(hs, order[r] + 1);
   }
-  unsigned err = 0;
-  CK(c, cudaMemcpy(&err, &c->st->err, sizeof(unsigned), cudaMemcpyDeviceToHost), "read error word");
-  if (err)
-    return c->fail(GS_EDEVICE, "device error word 0x%x (%s%s%s%s)", err,
-                   err & GS_DERR_LOOKBACK ? "sort look-back wait limit " : "",
-                   err & GS_DERR_STACK ? "walk stack " : "", err & GS_DERR_NODES ? "node pool " : "",
-                   err & GS_DERR_TREE ? "uploaded tree not BFS-contiguous" : "");
+  if (st > c->plan.sort_tiles || ft > c->plan.flag_tiles || gr > c->plan.groups ||
+      dc > c->plan.diag_chunks)
+    return c->fail(GS_EINVAL, "layout exceeds the pool's tile capacity");
+  CK(c, cudaStreamSynchronize(c->stream), "sync");
+  if (!h.empty()) {
+    CK(c, cudaMemcpy(c->segs, h.data(), sizeof(SegDesc) * h.size(), cudaMemcpyHostToDevice), "layout");
+    const uint32_t tot = std::max(st, std::max(ft, gr));
+    layout_maps_kernel<<<grid_for(tot, 256, 148 * 8), 256, 0, c->stream>>>(
+        c->segs, (uint32_t)h.size(), c->sort_map, st, c->flag_map, ft, c->group_map, gr);
+    CK(c, cudaGetLastError(), "layout maps");
+  }
+  Layout& L = c->lay;
+  L.segs = c->segs;
+  L.seg_of_sort_tile = c->sort_map;
+  L.seg_of_flag_tile = c->flag_map;
+  L.seg_of_group = c->group_map;
+  L.nseg = (uint32_t)h.size();
+  L.sort_tiles = st;
+  L.flag_tiles = ft;
+  L.groups = gr;
+  L.diag_chunks = dc;
+  c->hist_slots = hs;
+  c->seg_host = h;
+  c->walk_grid = std::min<uint32_t>(cdiv(gr, kWalkWarps), (uint32_t)c->sms * kWalkBlocksPerSM);
+  c->drop_graphs();
+  c->lay_dirty = false;
   return GS_OK;
+}
+
+// bbox, Morton frames and codes of `pos` (float4 records, stride in float4)
+// into keys[0], with the digit histograms of the sort.
+void enqueue_codes_sort(gs_ctx* c, const float4* pos, uint32_t stride, int advance_time) {
+  const Layout& L = c->lay;
+  cudaStream_t s = c->stream;
+  bbox_kernel<<<L.flag_tiles, kTileThreads, 0, s>>>(pos, stride, L, c->bbox_part, c->seg_ctr,
+                                                    c->frames, c->st, advance_time);
+  cudaMemsetAsync(c->sort_scratch, 0, sizeof(uint32_t) * (size_t)c->hist_slots * kSortPasses * 256, s);
+  cudaMemsetAsync(c->tile_ctr(), 0, sizeof(uint32_t) * (16 + (size_t)kSortPasses * L.sort_tiles * 256), s);
+  codes_kernel<<<L.flag_tiles, kTileThreads, 0, s>>>(pos, stride, L, c->frames, c->keys[0], c->hist(),
+                                                     kSortPasses);
+}
+
+// stable segmented sort of keys[0] -> keys[0] (sorted codes), vals[0] (gather
+// permutation) and, with inv, the inverse permutation.
+void enqueue_sort_passes(gs_ctx* c, bool inv) {
+  const Layout& L = c->lay;
+  cudaStream_t s = c->stream;
+  for (int p = 0; p < kSortPasses; p++) {
+    const int src = p & 1, dst = src ^ 1;
+    uint32_t* lb = c->lookback() + (size_t)p * L.sort_tiles * 256;
+    uint32_t* ctr = c->tile_ctr() + p;
+    if (p == 0)
+      onesweep_pass<true, false><<<L.sort_tiles, kSortThreads, 0, s>>>(
+          c->keys[src], nullptr, c->keys[dst], c->vals[dst], nullptr, c->hist(), p, lb, ctr, L, c->st);
+    else if (p < kSortPasses - 1)
+      onesweep_pass<false, false><<<L.sort_tiles, kSortThreads, 0, s>>>(
+          c->keys[src], c->vals[src], c->keys[dst], c->vals[dst], nullptr, c->hist(), p, lb, ctr, L,
+          c->st);
+    else
+      onesweep_pass<false, true><<<L.sort_tiles, kSortThreads, 0, s>>>(
+          c->keys[src], c->vals[src], c->keys[dst], c->vals[dst], inv ? c->inv : nullptr, c->hist(),
+          p, lb, ctr, L, c->st);
+  }
+}
+
+// the trees over keys[0] (sorted codes) with COM from pos; root size from the
+// Morton frames of the preceding sort (frames) or root_size.
+void enqueue_build(gs_ctx* c, const float4* pos, uint32_t stride, int com_mode, double root_size,
+                   const MortonFrame* frames) {
+  const Layout& L = c->lay;
+  cudaStream_t s = c->stream;
+  BuildBuffers b = c->bb();
+  tree_flags_kernel<<<L.flag_tiles, kFlagThreads, 0, s>>>(b, L);
+  tree_scan_kernel<<<L.nseg, kScanThreads, 0, s>>>(b, L, root_size, frames, c->st);
+  tree_emit_kernel<<<L.flag_tiles, kFlagThreads, 0, s>>>(b, L, c->st);
+  if (com_mode == kComJs)
+    tree_leaves_kernel<kComJs><<<L.flag_tiles, kLeafThreads, 0, s>>>(b, L, pos, stride, c->st);
+  else if (com_mode == kComF64)
+    tree_leaves_kernel<kComF64><<<L.flag_tiles, kLeafThreads, 0, s>>>(b, L, pos, stride, c->st);
+  else
+    tree_leaves_kernel<kComF32><<<L.flag_tiles, kLeafThreads, 0, s>>>(b, L, pos, stride, c->st);
 }
 
 void enqueue_walk(gs_ctx* c, int sf) {
@@ -316,42 +497,53 @@ void enqueue_walk(gs_ctx* c, int sf) {
   a.pin = c->part[c->cur];
   a.pout = c->part[c->cur ^ 1];
   a.stellar = c->stel[c->scur];
-  a.cm = c->ws.cm;
-  a.info = c->ws.info;
+  a.cm = c->cm;
+  a.info = c->info;
   a.st = c->st;
   a.energy = c->energy;
   a.dbg_acc = c->dbg_acc;
   a.dbg_dens = c->dbg_dens;
   a.partials = c->partials;
-  a.N = c->N;
-  a.node_cap = c->ws.cap;
   a.work = c->walk_work;
+  a.L = c->lay;
   const uint32_t g = c->walk_grid;
-  if (c->debug) {
-    if (sf) walk_kernel<true, true><<<g, kWalkThreads, 0, c->stream>>>(a);
-    else walk_kernel<false, true><<<g, kWalkThreads, 0, c->stream>>>(a);
-  } else {
-    if (sf) walk_kernel<true, false><<<g, kWalkThreads, 0, c->stream>>>(a);
-    else walk_kernel<false, false><<<g, kWalkThreads, 0, c->stream>>>(a);
+  cudaStream_t s = c->stream;
+  const bool one = c->lay.nseg == 1;
+  if (one) a.seg0 = c->seg_host[0];
+  else memset(&a.seg0, 0, sizeof(a.seg0));
+  const int v = (sf ? 1 : 0) | (c->debug ? 2 : 0) | (one ? 4 : 0);
+  switch (v) {
+    case 0: walk_kernel<false, false, false><<<g, kWalkThreads, 0, s>>>(a); break;
+    case 1: walk_kernel<true, false, false><<<g, kWalkThreads, 0, s>>>(a); break;
+    case 2: walk_kernel<false, true, false><<<g, kWalkThreads, 0, s>>>(a); break;
+    case 3: walk_kernel<true, true, false><<<g, kWalkThreads, 0, s>>>(a); break;
+    case 4: walk_kernel<false, false, true><<<g, kWalkThreads, 0, s>>>(a); break;
+    case 5: walk_kernel<true, false, true><<<g, kWalkThreads, 0, s>>>(a); break;
+    case 6: walk_kernel<false, true, true><<<g, kWalkThreads, 0, s>>>(a); break;
+    default: walk_kernel<true, true, true><<<g, kWalkThreads, 0, s>>>(a); break;
   }
+  // per-galaxy FP64 diagnostics of this walk
+  diag_reduce_kernel<<<c->lay.diag_chunks, dim3(32, kPartials), 0, s>>>(c->partials, c->lay, c->diag_chunk,
+                                                                         c->diag_ctr, c->diag_out);
   c->cur ^= 1;
 }
 
-// codes + sort + gather (+tracking/EMA) + build + refresh; flips cur and scur.
+// codes + sort + gather (+ tracking/EMA) + build + refresh; flips cur and scur.
 void enqueue_sort_build(gs_ctx* c, int advance_time) {
-  Workspace& w = c->ws;
-  enqueue_codes_sort(w, c->part[c->cur], 2, c->stream, c->st, advance_time);
-  gather_kernel<<<grid_for(c->N, 256, 148 * 16), 256, 0, c->stream>>>(
-      w.vals[0], c->part[c->cur], c->part[c->cur ^ 1], c->stel[c->scur], c->stel[c->scur ^ 1],
-      c->N, c->st, c->tracking ? 1 : 0);
+  const bool track = c->any_tracking();
+  const Layout& L = c->lay;
+  enqueue_codes_sort(c, c->part[c->cur], 2, advance_time);
+  enqueue_sort_passes(c, track);
+  gather_kernel<<<L.flag_tiles, kTileThreads, 0, c->stream>>>(
+      c->vals[0], c->part[c->cur], c->part[c->cur ^ 1], c->stel[c->scur], c->stel[c->scur ^ 1], L, c->st);
   c->cur ^= 1;
   c->scur ^= 1;
-  enqueue_build(w, c->part[c->cur], 2, w.cap, c->com_mode, 0.0, w.frame, c->stream, c->st, c->st);
-  c->tree = gs_ctx::kTreeBuilt;
+  if (track) track_kernel<<<cdiv(L.nseg, 128), 128, 0, c->stream>>>(c->inv, c->part[c->cur], L, c->st);
+  enqueue_build(c, c->part[c->cur], 2, c->com_mode, 0.0, c->frames);
 }
 
-// After a Params upload: sim_time follows Params.time, and tracked halo centres
-// keep their device-side smoothed values.
+// After a Params upload: sim_time follows Params.time, N is the galaxy's, and
+// tracked halo centres keep their device-side smoothed values.
 __global__ void params_fixup_kernel(DevState* st, uint32_t N) {
   st->p.N = N;
   st->sim_time = (double)st->p.time;
@@ -362,18 +554,18 @@ __global__ void params_fixup_kernel(DevState* st, uint32_t N) {
   }
 }
 
+// c0/c1: pool indices or -1.
 __global__ void tracking_init_kernel(DevState* st, const float4* P, long long c0, long long c1,
                                      int have0, double h0x, double h0y, double h0z, int have1,
-                                     double h1x, double h1y, double h1z, uint32_t N) {
+                                     double h1x, double h1y, double h1z) {
   const long long c[2] = {c0, c1};
   const int have[2] = {have0, have1};
   const double hv[2][3] = {{h0x, h0y, h0z}, {h1x, h1y, h1z}};
   for (int h = 0; h < 2; h++) {
     st->central[h] = c[h];
-    st->central_next[h] = c[h];
     if (have[h]) {
       for (int k = 0; k < 3; k++) st->halo_c[h][k] = hv[h][k];
-    } else if (c[h] >= 0 && c[h] < (long long)N) {
+    } else if (c[h] >= 0) {
       const float4 p = P[2 * (size_t)c[h]];
       st->halo_c[h][0] = p.x;
       st->halo_c[h][1] = p.y;
@@ -396,6 +588,100 @@ __global__ void bh_patch_kernel(gs_node* bh, const float4* cm, uint32_t n) {
   }
 }
 
+// applyPermutation of one galaxy (pointers at its offset; perm galaxy-local and
+// checked on the host): out[i] = in[perm[i]] (nbody_bh.wgsl:322-326, :336-340).
+__global__ void gather_range_kernel(const uint32_t* __restrict__ perm, const float4* __restrict__ pin,
+                                    float4* __restrict__ pout, const float4* __restrict__ sin,
+                                    float4* __restrict__ sout, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t s = perm[i];
+    if (s >= n) continue;
+    pout[2 * (size_t)i] = pin[2 * (size_t)s];
+    pout[2 * (size_t)i + 1] = pin[2 * (size_t)s + 1];
+    sout[i] = sin[s];
+  }
+}
+
+int wait_stream(gs_ctx* c, uint64_t timeout_ns, const Slot* s) {
+  CK(c, cudaEventRecord(c->ev, c->stream), "cudaEventRecord");
+  if (timeout_ns == 0) {
+    CK(c, cudaEventSynchronize(c->ev), "cudaEventSynchronize");
+  } else {
+    const auto t0 = std::chrono::steady_clock::now();
+    while (true) {
+      cudaError_t q = cudaEventQuery(c->ev);
+      if (q == cudaSuccess) break;
+      if (q != cudaErrorNotReady) return c->cuda(q, "cudaEventQuery");
+      const auto dt = std::chrono::duration_cast<std::chrono::nanoseconds>(
+                          std::chrono::steady_clock::now() - t0)
+                          .count();
+      if ((uint64_t)dt > timeout_ns)
+        return c->fail(GS_ETIMEDOUT, "stream did not drain within %llu ns",
+                       (unsigned long long)timeout_ns);
+      std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+  }
+  // error words: the given slot's, or every live slot's
+  unsigned err = 0;
+  for (uint32_t k = 0; k < c->slots.size(); k++) {
+    if (s ? (&c->slots[k] != s) : !c->slots[k].live) continue;
+    unsigned e = 0;
+    CK(c, cudaMemcpy(&e, &c->st[k].err, sizeof(unsigned), cudaMemcpyDeviceToHost), "read error word");
+    err |= e;
+  }
+  if (err)
+    return c->fail(GS_EDEVICE, "device error word 0x%x (%s%s%s%s)", err,
+                   err & GS_DERR_LOOKBACK ? "sort look-back wait limit " : "",
+                   err & GS_DERR_STACK ? "walk stack " : "", err & GS_DERR_NODES ? "node pool " : "",
+                   err & GS_DERR_TREE ? "uploaded tree not BFS-contiguous" : "");
+  return GS_OK;
+}
+
+int stage_grow(gs_ctx* c, uint32_t need_nodes) {
+  if (c->bh && c->max_bh >= need_nodes) return GS_OK;
+  gs_node* p = nullptr;
+  CK(c, c->alloc(&p, std::max<uint32_t>(need_nodes, 1)), "bh staging");
+  c->bh = p;  // the old staging stays owned until the context is destroyed
+  c->max_bh = need_nodes;
+  return GS_OK;
+}
+
+// Put a galaxy into slot `slot` at pool offset off (both ping-pongs written).
+int slot_fill(gs_ctx* c, uint32_t slot, uint32_t off, uint32_t span, uint32_t n, uint32_t node_cap,
+              const float* particles8, const float* stellar4, const gs_params* params) {
+  Slot& s = c->slots[slot];
+  CK(c, cudaStreamSynchronize(c->stream), "sync");
+  const size_t pb = (size_t)n * 32, sb = (size_t)n * 16;
+  for (int k = 0; k < 2; k++) {
+    CK(c, cudaMemcpy(c->part[k] + 2 * (size_t)off, particles8, pb, cudaMemcpyHostToDevice), "upload");
+    if (stellar4)
+      CK(c, cudaMemcpy(c->stel[k] + off, stellar4, sb, cudaMemcpyHostToDevice), "upload");
+    else
+      CK(c, cudaMemset(c->stel[k] + off, 0, sb), "memset");
+  }
+  CK(c, cudaMemset(c->cm + 2 * (size_t)off, 0, sizeof(float4) * node_cap), "memset");
+  CK(c, cudaMemset(c->info + 2 * (size_t)off, 0, sizeof(WalkInfo) * node_cap), "memset");
+  CK(c, cudaMemset(c->meta + slot, 0, sizeof(TreeMeta)), "memset");
+  CK(c, cudaMemset(c->diag_out + (size_t)slot * kPartials, 0, sizeof(double) * kPartials), "memset");
+  DevState st0;
+  memset(&st0, 0, sizeof(st0));
+  if (params) st0.p = *params;
+  st0.p.N = n;
+  st0.sim_time = (double)st0.p.time;
+  st0.central[0] = st0.central[1] = -1;
+  CK(c, cudaMemcpy(c->st + slot, &st0, sizeof(st0), cudaMemcpyHostToDevice), "state");
+  s = Slot();
+  s.live = true;
+  s.off = off;
+  s.span = span;
+  s.n = n;
+  s.node_off = 2 * off;
+  s.node_cap = node_cap;
+  s.hp = st0.p;
+  c->lay_dirty = true;
+  return GS_OK;
+}
+
 int host_pack4(const float* src, uint32_t N, uint32_t stride, std::vector<float4>& out) {
   out.resize(N);
   for (uint32_t i = 0; i < N; i++)
@@ -406,17 +692,14 @@ int host_pack4(const float* src, uint32_t N, uint32_t stride, std::vector<float4
 
 }  // namespace
 
-extern "C" {
-
-const char* gs_last_error(const gs_ctx* ctx) { return ctx ? ctx->err : g_err; }
-
-}  // extern "C"
-
 // Context-free error text for entry points defined in other translation units.
 void gs_internal_set_error(const char* msg) { set_err(g_err, "%s", msg); }
 
 extern "C" {
-const char* gs_version(void) { return "galaxy_b200 0.1 (sm_100a)"; }
+
+const char* gs_last_error(const gs_ctx* ctx) { return ctx ? ctx->err : g_err; }
+
+const char* gs_version(void) { return "galaxy_b200 0.2 (sm_100a)"; }
 
 int gs_device_count(int* count) {
   if (!count) return GS_EINVAL;
@@ -429,19 +712,38 @@ int gs_device_count(int* count) {
   return GS_OK;
 }
 
-int gs_create_on(int device, uint32_t N, const float* particles8, const float* stellar4,
-                 gs_ctx** out) {
+// ---- pools ---------------------------------------------------------------------------
+
+int gs_device_memory(int device, uint64_t* free_bytes, uint64_t* total_bytes) {
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaError_t e = cudaSetDevice(device);
+  size_t f = 0, t = 0;
+  if (e == cudaSuccess) e = cudaMemGetInfo(&f, &t);
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) {
+    set_err(g_err, "cudaMemGetInfo: %s", cudaGetErrorString(e));
+    return GS_ECUDA;
+  }
+  if (free_bytes) *free_bytes = f;
+  if (total_bytes) *total_bytes = t;
+  return GS_OK;
+}
+
+uint64_t gs_pool_bytes(uint64_t particle_capacity, uint32_t max_galaxies) {
+  return plan_bytes(make_plan(particle_capacity, max_galaxies));
+}
+
+int gs_pool_create(int device, uint64_t particle_capacity, uint32_t max_galaxies, gs_ctx** out) {
   if (!out) {
     set_err(g_err, "out is NULL");
     return GS_EINVAL;
   }
   *out = nullptr;
-  if (N == 0 || N > kMaxN) {
-    set_err(g_err, "N must be in [1, %u], got %u", kMaxN, N);
-    return GS_EINVAL;
-  }
-  if (!particles8) {
-    set_err(g_err, "particles8 is NULL");
+  if (particle_capacity == 0 || particle_capacity > kMaxPool || max_galaxies == 0 ||
+      max_galaxies > kMaxSlots) {
+    set_err(g_err, "pool capacity must be in [1, %llu] particles and [1, %u] galaxies",
+            (unsigned long long)kMaxPool, kMaxSlots);
     return GS_EINVAL;
   }
   int ndev = 0;
@@ -451,66 +753,124 @@ int gs_create_on(int device, uint32_t N, const float* particles8, const float* s
   }
   gs_ctx* c = new (std::nothrow) gs_ctx();
   if (!c) return GS_ENOMEM;
-  c->device = device;
-  c->N = N;
-  cudaSetDevice(device);
-  auto bail = [&](int rc) {
+  const int rc = pool_init(c, device, particle_capacity, max_galaxies);
+  if (rc) {
     set_err(g_err, "%s", c->err);
     gs_destroy(c);
     return rc;
-  };
-  int rc;
-  if ((rc = c->cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream")))
-    return bail(rc);
-  if ((rc = c->cuda(cudaEventCreateWithFlags(&c->ev, cudaEventDisableTiming), "event")))
-    return bail(rc);
-  if ((rc = c->cuda(c->ws.init(N), "workspace"))) return bail(rc);
-  Workspace& w = c->ws;
-  if ((rc = c->cuda(w.alloc(&c->part[0], 2 * (size_t)N), "particles"))) return bail(rc);
-  if ((rc = c->cuda(w.alloc(&c->part[1], 2 * (size_t)N), "particles"))) return bail(rc);
-  if ((rc = c->cuda(w.alloc(&c->stel[0], N), "stellar"))) return bail(rc);
-  if ((rc = c->cuda(w.alloc(&c->stel[1], N), "stellar"))) return bail(rc);
-  if ((rc = c->cuda(w.alloc(&c->energy, N), "energy"))) return bail(rc);
-  if ((rc = c->cuda(w.alloc(&c->compact, N), "compact"))) return bail(rc);
-  if ((rc = c->cuda(w.alloc(&c->perm_user, N), "perm"))) return bail(rc);
-  if ((rc = c->cuda(w.alloc(&c->st, 1), "state"))) return bail(rc);
-  c->walk_groups = cdiv(N, kWalkGroup);
-  {
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    c->walk_grid = std::min<uint32_t>(cdiv(c->walk_groups, kWalkWarps),
-                                      (uint32_t)sms * kWalkBlocksPerSM);
   }
-  if ((rc = c->cuda(w.alloc(&c->partials, (size_t)c->walk_groups * kPartials), "partials")))
-    return bail(rc);
-  if ((rc = c->cuda(w.alloc(&c->walk_work, 4), "walk counters"))) return bail(rc);
-  if ((rc = c->cuda(cudaMemset(c->walk_work, 0, 16), "walk counters"))) return bail(rc);
-  if ((rc = c->cuda(w.alloc(&c->diag_out, 8), "diag"))) return bail(rc);
-  if ((rc = c->cuda(cudaMallocHost(&c->host_stage, (size_t)N * 16 + 256), "pinned stage")))
-    return bail(rc);
-  const size_t pb = (size_t)N * 32, sb = (size_t)N * 16;
-  if ((rc = c->cuda(cudaMemcpy(c->part[0], particles8, pb, cudaMemcpyHostToDevice), "upload")))
-    return bail(rc);
-  if ((rc = c->cuda(cudaMemcpy(c->part[1], particles8, pb, cudaMemcpyHostToDevice), "upload")))
-    return bail(rc);
-  for (int k = 0; k < 2; k++) {
-    if (stellar4)
-      rc = c->cuda(cudaMemcpy(c->stel[k], stellar4, sb, cudaMemcpyHostToDevice), "upload");
-    else
-      rc = c->cuda(cudaMemset(c->stel[k], 0, sb), "memset");
-    if (rc) return bail(rc);
-  }
-  DevState st0;
-  memset(&st0, 0, sizeof(st0));
-  st0.p.N = N;
-  st0.central[0] = st0.central[1] = -1;
-  st0.central_next[0] = st0.central_next[1] = -1;
-  c->hp = st0.p;
-  if ((rc = c->cuda(cudaMemcpy(c->st, &st0, sizeof(st0), cudaMemcpyHostToDevice), "state")))
-    return bail(rc);
-  if ((rc = c->cuda(cudaMemset(c->partials, 0, sizeof(double) * c->walk_groups * kPartials), "m")))
-    return bail(rc);
   *out = c;
+  return GS_OK;
+}
+
+int gs_pool_add(gs_ctx* ctx, uint32_t N, const float* particles8, const float* stellar4,
+                const gs_params* params, uint32_t* slot_out) {
+  CTX_CHECK(ctx);
+  if (N == 0 || !particles8) return ctx->fail(GS_EINVAL, "N must be >= 1 and particles8 set");
+  if (ctx->single) return ctx->fail(GS_EINVAL, "a single-galaxy context takes no more galaxies");
+  uint32_t slot = 0;
+  while (slot < ctx->slots.size() && ctx->slots[slot].live) slot++;
+  if (slot == ctx->slots.size()) return ctx->fail(GS_ENOMEM, "no free galaxy slot");
+  const uint64_t span = (uint64_t)cdiv(N, kAlign) * kAlign;
+  uint64_t off = 0;
+  if (!ctx->palloc.alloc(span, &off))
+    return ctx->fail(GS_ENOMEM, "no free particle range of %llu in the pool", (unsigned long long)span);
+  int rc = slot_fill(ctx, slot, (uint32_t)off, (uint32_t)span, N, 2 * N, particles8, stellar4, params);
+  if (rc) {
+    ctx->palloc.release(off, span);
+    ctx->slots[slot].live = false;
+    return rc;
+  }
+  if (slot_out) *slot_out = slot;
+  return GS_OK;
+}
+
+int gs_pool_remove(gs_ctx* ctx, uint32_t slot) {
+  CTX_CHECK(ctx);
+  if (slot >= ctx->slots.size() || !ctx->slots[slot].live)
+    return ctx->fail(GS_EINVAL, "slot %u holds no galaxy", slot);
+  CK(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+  Slot& s = ctx->slots[slot];
+  ctx->palloc.release(s.off, s.span);
+  s = Slot();
+  ctx->lay_dirty = true;
+  return GS_OK;
+}
+
+int gs_pool_free(gs_ctx* ctx, uint64_t* largest_range, uint32_t* free_slots) {
+  CTX_CHECK(ctx);
+  if (largest_range) *largest_range = ctx->palloc.largest();
+  if (free_slots) {
+    uint32_t f = 0;
+    for (const Slot& s : ctx->slots) f += s.live ? 0 : 1;
+    *free_slots = f;
+  }
+  return GS_OK;
+}
+
+int gs_select(gs_ctx* ctx, uint32_t slot) {
+  CTX_CHECK(ctx);
+  if (slot >= ctx->slots.size()) return ctx->fail(GS_EINVAL, "slot %u out of range", slot);
+  ctx->sel = slot;
+  return GS_OK;
+}
+
+int gs_pool_energies(gs_ctx* ctx, gs_diag* out, uint32_t cap) {
+  CTX_CHECK(ctx);
+  if (!out) return ctx->fail(GS_EINVAL, "out is NULL");
+  const uint32_t n = std::min<uint32_t>(cap, (uint32_t)ctx->slots.size());
+  std::vector<double> h((size_t)n * kPartials);
+  if (n)
+    CK(ctx, cudaMemcpyAsync(h.data(), ctx->diag_out, sizeof(double) * h.size(), cudaMemcpyDeviceToHost,
+                            ctx->stream),
+       "diag");
+  int rc = wait_stream(ctx, 0, nullptr);
+  if (rc) return rc;
+  for (uint32_t k = 0; k < n; k++) {
+    const double* v = &h[(size_t)k * kPartials];
+    if (!ctx->slots[k].live) {
+      memset(&out[k], 0, sizeof(gs_diag));
+      continue;
+    }
+    out[k].e_diag = v[0];
+    out[k].e_true = v[1];
+    out[k].momentum[0] = v[2];
+    out[k].momentum[1] = v[3];
+    out[k].momentum[2] = v[4];
+    out[k].mass = v[5];
+  }
+  return GS_OK;
+}
+
+// ---- NBodyGPU surface ------------------------------------------------------------------
+
+int gs_create_on(int device, uint32_t N, const float* particles8, const float* stellar4,
+                 gs_ctx** out) {
+  if (!out) {
+    set_err(g_err, "out is NULL");
+    return GS_EINVAL;
+  }
+  *out = nullptr;
+  if (N == 0 || N > kMaxPool) {
+    set_err(g_err, "N must be in [1, %llu], got %u", (unsigned long long)kMaxPool, N);
+    return GS_EINVAL;
+  }
+  if (!particles8) {
+    set_err(g_err, "particles8 is NULL");
+    return GS_EINVAL;
+  }
+  int rc = gs_pool_create(device, N, 1, out);
+  if (rc) return rc;
+  gs_ctx* c = *out;
+  rc = slot_fill(c, 0, 0, N, N, 2 * N + 4096, particles8, stellar4, nullptr);
+  if (rc) {
+    set_err(g_err, "%s", c->err);
+    gs_destroy(c);
+    *out = nullptr;
+    return rc;
+  }
+  c->palloc.init(0);
+  c->single = true;
   return GS_OK;
 }
 
@@ -522,47 +882,46 @@ int gs_create(uint32_t N, const float* particles8, const float* stellar4, gs_ctx
 
 int gs_destroy(gs_ctx* ctx) {
   if (!ctx) return GS_OK;
-  cudaSetDevice(ctx->device);
-  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  ctx->drop_graphs();
-  ctx->ws.release();
-  if (ctx->host_stage) cudaFreeHost(ctx->host_stage);
-  if (ctx->ev) cudaEventDestroy(ctx->ev);
-  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  pool_release(ctx);
   delete ctx;
   return GS_OK;
 }
 
 int gs_update_params(gs_ctx* ctx, const gs_params* params) {
   CTX_CHECK(ctx);
+  SLOT(ctx, s);
   if (!params) return ctx->fail(GS_EINVAL, "params is NULL");
-  ctx->hp = *params;
-  ctx->hp.N = ctx->N;
+  s->hp = *params;
+  s->hp.N = s->n;
   // the 96-byte uniform goes through pinned memory so the async copy never
   // reads a caller buffer after return
-  gs_params* stage = reinterpret_cast<gs_params*>(static_cast<char*>(ctx->host_stage) + (size_t)ctx->N * 16);
+  gs_params* stage = reinterpret_cast<gs_params*>(ctx->host_stage) + ctx->sel;
   CK(ctx, cudaStreamSynchronize(ctx->stream), "sync");
-  *stage = ctx->hp;
-  CK(ctx, cudaMemcpyAsync(&ctx->st->p, stage, sizeof(gs_params), cudaMemcpyHostToDevice, ctx->stream),
+  *stage = s->hp;
+  DevState* st = ctx->st + ctx->sel;
+  CK(ctx, cudaMemcpyAsync(&st->p, stage, sizeof(gs_params), cudaMemcpyHostToDevice, ctx->stream),
      "params upload");
-  params_fixup_kernel<<<1, 1, 0, ctx->stream>>>(ctx->st, ctx->N);
+  params_fixup_kernel<<<1, 1, 0, ctx->stream>>>(st, s->n);
   CK(ctx, cudaGetLastError(), "params fixup");
   return GS_OK;
 }
 
 int gs_set_time(gs_ctx* ctx, double t) {
   CTX_CHECK(ctx);
+  SLOT(ctx, s);
+  (void)s;
   CK(ctx, cudaStreamSynchronize(ctx->stream), "sync");
-  CK(ctx, cudaMemcpy(&ctx->st->sim_time, &t, sizeof(double), cudaMemcpyHostToDevice), "time");
+  CK(ctx, cudaMemcpy(&ctx->st[ctx->sel].sim_time, &t, sizeof(double), cudaMemcpyHostToDevice), "time");
   return GS_OK;
 }
 
 int gs_update_central_mass(gs_ctx* ctx, float mass, uint32_t idx) {
   CTX_CHECK(ctx);
-  if (idx >= ctx->N) return ctx->fail(GS_EINVAL, "central index %u >= N %u", idx, ctx->N);
+  SLOT(ctx, s);
+  if (idx >= s->n) return ctx->fail(GS_EINVAL, "central index %u >= N %u", idx, s->n);
   CK(ctx, cudaStreamSynchronize(ctx->stream), "sync");
   for (int k = 0; k < 2; k++)
-    CK(ctx, cudaMemcpy(reinterpret_cast<char*>(ctx->part[k]) + (size_t)idx * 32 + 12, &mass, 4,
+    CK(ctx, cudaMemcpy(reinterpret_cast<char*>(ctx->part[k]) + ((size_t)s->off + idx) * 32 + 12, &mass, 4,
                        cudaMemcpyHostToDevice),
        "central mass");
   return GS_OK;
@@ -570,19 +929,32 @@ int gs_update_central_mass(gs_ctx* ctx, float mass, uint32_t idx) {
 
 int gs_apply_permutation(gs_ctx* ctx, const uint32_t* perm) {
   CTX_CHECK(ctx);
+  SLOT(ctx, s);
   if (!perm) return ctx->fail(GS_EINVAL, "perm is NULL");
-  for (uint32_t i = 0; i < ctx->N; i++)
-    if (perm[i] >= ctx->N) return ctx->fail(GS_EINVAL, "perm[%u] = %u out of range", i, perm[i]);
+  for (uint32_t i = 0; i < s->n; i++)
+    if (perm[i] >= s->n) return ctx->fail(GS_EINVAL, "perm[%u] = %u out of range", i, perm[i]);
   CK(ctx, cudaStreamSynchronize(ctx->stream), "sync");
-  CK(ctx, cudaMemcpyAsync(ctx->perm_user, perm, sizeof(uint32_t) * ctx->N, cudaMemcpyHostToDevice,
+  CK(ctx, cudaMemcpyAsync(ctx->perm_user + s->off, perm, sizeof(uint32_t) * s->n, cudaMemcpyHostToDevice,
                           ctx->stream),
      "perm upload");
-  gather_kernel<<<grid_for(ctx->N, 256, 148 * 16), 256, 0, ctx->stream>>>(
-      ctx->perm_user, ctx->part[ctx->cur], ctx->part[ctx->cur ^ 1], ctx->stel[ctx->scur],
-      ctx->stel[ctx->scur ^ 1], ctx->N, ctx->st, 0);
+  const int c0 = ctx->cur, s0 = ctx->scur;
+  gather_range_kernel<<<grid_for(s->n, 256, 148 * 16), 256, 0, ctx->stream>>>(
+      ctx->perm_user + s->off, ctx->part[c0] + 2 * (size_t)s->off, ctx->part[c0 ^ 1] + 2 * (size_t)s->off,
+      ctx->stel[s0] + s->off, ctx->stel[s0 ^ 1] + s->off, s->n);
   CK(ctx, cudaGetLastError(), "gather");
-  ctx->cur ^= 1;
-  ctx->scur ^= 1;
+  int live = 0;
+  for (const Slot& q : ctx->slots) live += q.live ? 1 : 0;
+  if (live == 1) {
+    ctx->cur ^= 1;  // NBodyGPU.js:328 flips the ping-pongs
+    ctx->scur ^= 1;
+  } else {  // other galaxies share the buffers: copy the result back instead
+    CK(ctx, cudaMemcpyAsync(ctx->part[c0] + 2 * (size_t)s->off, ctx->part[c0 ^ 1] + 2 * (size_t)s->off,
+                            (size_t)s->n * 32, cudaMemcpyDeviceToDevice, ctx->stream),
+       "copy back");
+    CK(ctx, cudaMemcpyAsync(ctx->stel[s0] + s->off, ctx->stel[s0 ^ 1] + s->off, (size_t)s->n * 16,
+                            cudaMemcpyDeviceToDevice, ctx->stream),
+       "copy back");
+  }
   CK(ctx, cudaStreamSynchronize(ctx->stream), "sync");
   return GS_OK;
 }
@@ -590,46 +962,59 @@ int gs_apply_permutation(gs_ctx* ctx, const uint32_t* perm) {
 int gs_upload_tree(gs_ctx* ctx, const gs_node* nodes, uint32_t num_nodes,
                    const uint32_t* level_ranges, uint32_t n_levels) {
   CTX_CHECK(ctx);
+  SLOT(ctx, s);
   if (!nodes && num_nodes) return ctx->fail(GS_EINVAL, "nodes is NULL");
-  const uint32_t max_bh = 4 * ctx->N + 1024;  // NBodyGPU.js:58
+  const uint32_t max_bh = 4 * s->n + 1024;  // NBodyGPU.js:58
   const uint32_t n = std::min(num_nodes, max_bh);
-  if (n > ctx->ws.cap)
-    return ctx->fail(GS_EINVAL, "tree of %u nodes exceeds the pool of %u", n, ctx->ws.cap);
-  if (!ctx->bh) {
-    CK(ctx, ctx->ws.alloc(&ctx->bh, ctx->ws.cap), "bh staging");
-    ctx->max_bh = ctx->ws.cap;
-  }
+  if (n > s->node_cap)
+    return ctx->fail(GS_EINVAL, "tree of %u nodes exceeds the galaxy's pool of %u", n, s->node_cap);
+  int rc = stage_grow(ctx, n);
+  if (rc) return rc;
   CK(ctx, cudaStreamSynchronize(ctx->stream), "sync");
   if (n) CK(ctx, cudaMemcpy(ctx->bh, nodes, (size_t)n * sizeof(gs_node), cudaMemcpyHostToDevice), "tree");
+  // the build's leaves pass skips this galaxy until its next on-device build
+  CK(ctx, cudaMemsetAsync(ctx->meta + ctx->sel, 0, sizeof(TreeMeta), ctx->stream), "meta");
   if (n)
     upload_convert_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, ctx->stream>>>(
-        ctx->bh, n, ctx->N, ctx->ws.cm, ctx->ws.info, ctx->st);
+        ctx->bh, n, s->n, s->node_off, s->off, ctx->cm, ctx->info, ctx->st + ctx->sel);
   CK(ctx, cudaGetLastError(), "convert");
-  if (level_ranges) {
-    ctx->up_lr.assign(level_ranges, level_ranges + 2 * std::min<uint32_t>(n_levels, 16));
-  }
-  ctx->up_nodes = n;
-  ctx->tree = gs_ctx::kTreeUploaded;
-  return wait_stream(ctx, 0);
+  s->up_lr.clear();
+  if (level_ranges) s->up_lr.assign(level_ranges, level_ranges + 2 * std::min<uint32_t>(n_levels, 16));
+  s->up_nodes = n;
+  s->up_host.assign(nodes, nodes + n);
+  s->tree = Slot::kTreeUploaded;
+  return wait_stream(ctx, 0, s);
 }
 
 int gs_refresh(gs_ctx* ctx) {
   CTX_CHECK(ctx);
-  if (ctx->tree == gs_ctx::kTreeUploaded) {
-    if (ctx->up_lr.empty()) return GS_OK;  // NBodyGPU.js:309 no-op without levelRanges
-    for (int64_t l = (int64_t)ctx->up_lr.size() / 2 - 1; l >= 0; l--) {
-      const uint32_t start = ctx->up_lr[2 * l], count = ctx->up_lr[2 * l + 1];
+  int rc = ensure_layout(ctx);
+  if (rc) return rc;
+  bool built = false;
+  for (Slot& s : ctx->slots) {
+    if (!s.live) continue;
+    if (s.tree == Slot::kTreeBuilt) built = true;
+    if (s.tree != Slot::kTreeUploaded) continue;
+    // NBodyGPU.js:309: no-op without levelRanges; deepest level first
+    for (int64_t l = (int64_t)s.up_lr.size() / 2 - 1; l >= 0; l--) {
+      const uint32_t start = s.up_lr[2 * l], count = s.up_lr[2 * l + 1];
       if (!count) continue;
-      if ((uint64_t)start + count > ctx->up_nodes)
-        return ctx->fail(GS_EINVAL, "level %lld [%u, +%u) beyond %u nodes", (long long)l, start,
-                         count, ctx->up_nodes);
-      refresh_level_kernel<<<cdiv(count, 64), 64, 0, ctx->stream>>>(ctx->part[ctx->cur], ctx->ws.cm,
-                                                                     ctx->ws.info, start, count);
+      if ((uint64_t)start + count > s.up_nodes)
+        return ctx->fail(GS_EINVAL, "level %lld [%u, +%u) beyond %u nodes", (long long)l, start, count,
+                         s.up_nodes);
+      refresh_level_kernel<<<cdiv(count, 64), 64, 0, ctx->stream>>>(ctx->part[ctx->cur], ctx->cm, ctx->info,
+                                                                     s.node_off + start, count);
     }
-  } else if (ctx->tree == gs_ctx::kTreeBuilt) {
-    BuildBuffers b = ctx->ws.bb(ctx->ws.cap);
-    tree_leaves_kernel<kComF32><<<grid_for(ctx->N, 256, 148 * 16), 256, 0, ctx->stream>>>(
-        b, ctx->part[ctx->cur], 2, ctx->st);
+  }
+  if (built && ctx->lay.nseg) {
+    BuildBuffers b = ctx->bb();
+    const Layout& L = ctx->lay;
+    if (ctx->com_mode == kComF64)
+      tree_leaves_kernel<kComF64><<<L.flag_tiles, kLeafThreads, 0, ctx->stream>>>(b, L, ctx->part[ctx->cur], 2,
+                                                                                   ctx->st);
+    else
+      tree_leaves_kernel<kComF32><<<L.flag_tiles, kLeafThreads, 0, ctx->stream>>>(b, L, ctx->part[ctx->cur], 2,
+                                                                                   ctx->st);
   }
   CK(ctx, cudaGetLastError(), "refresh");
   return GS_OK;
@@ -637,6 +1022,9 @@ int gs_refresh(gs_ctx* ctx) {
 
 int gs_step(gs_ctx* ctx) {
   CTX_CHECK(ctx);
+  int rc = ensure_layout(ctx);
+  if (rc) return rc;
+  if (!ctx->lay.nseg) return GS_OK;
   enqueue_walk(ctx, 0);
   CK(ctx, cudaGetLastError(), "walk");
   return GS_OK;
@@ -644,73 +1032,82 @@ int gs_step(gs_ctx* ctx) {
 
 int gs_star_formation(gs_ctx* ctx) {
   CTX_CHECK(ctx);
-  sf_kernel<<<grid_for(ctx->N, 256, 148 * 16), 256, 0, ctx->stream>>>(ctx->part[ctx->cur],
-                                                                      ctx->stel[ctx->scur], ctx->N,
-                                                                      ctx->st);
+  int rc = ensure_layout(ctx);
+  if (rc) return rc;
+  if (!ctx->lay.nseg) return GS_OK;
+  sf_kernel<<<ctx->lay.flag_tiles, kTileThreads, 0, ctx->stream>>>(ctx->part[ctx->cur], ctx->stel[ctx->scur],
+                                                                    ctx->lay, ctx->st);
   CK(ctx, cudaGetLastError(), "star formation");
   return GS_OK;
 }
 
 int gs_read_positions(gs_ctx* ctx, float* out4, uint64_t timeout_ns) {
   CTX_CHECK(ctx);
+  SLOT(ctx, s);
   if (!out4) return ctx->fail(GS_EINVAL, "out4 is NULL");
-  compact_kernel<<<grid_for(ctx->N, 256, 148 * 16), 256, 0, ctx->stream>>>(
-      ctx->part[ctx->cur], ctx->energy, ctx->compact, ctx->N);
+  compact_kernel<<<grid_for(s->n, 256, 148 * 16), 256, 0, ctx->stream>>>(
+      ctx->part[ctx->cur] + 2 * (size_t)s->off, ctx->energy + s->off, ctx->compact + s->off, s->n);
   CK(ctx, cudaGetLastError(), "compact");
-  CK(ctx, cudaMemcpyAsync(ctx->host_stage, ctx->compact, (size_t)ctx->N * 16, cudaMemcpyDeviceToHost,
-                          ctx->stream),
-     "readback");
-  int rc = wait_stream(ctx, timeout_ns);
+  int rc = wait_stream(ctx, timeout_ns, s);
   if (rc) return rc;
-  memcpy(out4, ctx->host_stage, (size_t)ctx->N * 16);
+  CK(ctx, cudaMemcpy(out4, ctx->compact + s->off, (size_t)s->n * 16, cudaMemcpyDeviceToHost), "readback");
   return GS_OK;
 }
 
 int gs_position_buffer(gs_ctx* ctx, void** dptr) {
   CTX_CHECK(ctx);
+  SLOT(ctx, s);
   if (!dptr) return ctx->fail(GS_EINVAL, "dptr is NULL");
-  *dptr = ctx->part[ctx->cur];
+  *dptr = ctx->part[ctx->cur] + 2 * (size_t)s->off;
   return GS_OK;
 }
 
 int gs_stellar_buffer(gs_ctx* ctx, void** dptr) {
   CTX_CHECK(ctx);
+  SLOT(ctx, s);
   if (!dptr) return ctx->fail(GS_EINVAL, "dptr is NULL");
-  *dptr = ctx->stel[ctx->scur];
+  *dptr = ctx->stel[ctx->scur] + s->off;
   return GS_OK;
 }
 
 int gs_set_tracking(gs_ctx* ctx, int64_t c1, int64_t c2, const double* h1, const double* h2) {
   CTX_CHECK(ctx);
-  if (c1 >= (int64_t)ctx->N || c2 >= (int64_t)ctx->N)
-    return ctx->fail(GS_EINVAL, "tracked index out of range");
-  ctx->tracking = c1 >= 0 || c2 >= 0;
+  SLOT(ctx, s);
+  if (c1 >= (int64_t)s->n || c2 >= (int64_t)s->n) return ctx->fail(GS_EINVAL, "tracked index out of range");
+  const bool was = ctx->any_tracking();
+  s->tracking = c1 >= 0 || c2 >= 0;
   tracking_init_kernel<<<1, 1, 0, ctx->stream>>>(
-      ctx->st, ctx->part[ctx->cur], c1 < 0 ? -1 : c1, c2 < 0 ? -1 : c2, h1 != nullptr,
-      h1 ? h1[0] : 0, h1 ? h1[1] : 0, h1 ? h1[2] : 0, h2 != nullptr, h2 ? h2[0] : 0,
-      h2 ? h2[1] : 0, h2 ? h2[2] : 0, ctx->N);
+      ctx->st + ctx->sel, ctx->part[ctx->cur], c1 < 0 ? -1 : s->off + c1, c2 < 0 ? -1 : s->off + c2,
+      h1 != nullptr, h1 ? h1[0] : 0, h1 ? h1[1] : 0, h1 ? h1[2] : 0, h2 != nullptr, h2 ? h2[0] : 0,
+      h2 ? h2[1] : 0, h2 ? h2[2] : 0);
   CK(ctx, cudaGetLastError(), "tracking");
-  ctx->drop_graphs();
-  return wait_stream(ctx, 0);
+  if (was != ctx->any_tracking()) ctx->drop_graphs();
+  return wait_stream(ctx, 0, s);
 }
 
 int gs_get_tracking(gs_ctx* ctx, int64_t* c1, int64_t* c2, double* h1, double* h2) {
   CTX_CHECK(ctx);
-  int rc = wait_stream(ctx, 0);
+  SLOT(ctx, s);
+  int rc = wait_stream(ctx, 0, s);
   if (rc) return rc;
-  DevState s;
-  CK(ctx, cudaMemcpy(&s, ctx->st, sizeof(s), cudaMemcpyDeviceToHost), "state");
-  if (c1) *c1 = s.central[0];
-  if (c2) *c2 = s.central[1];
-  if (h1) memcpy(h1, s.halo_c[0], 3 * sizeof(double));
-  if (h2) memcpy(h2, s.halo_c[1], 3 * sizeof(double));
+  DevState d;
+  CK(ctx, cudaMemcpy(&d, ctx->st + ctx->sel, sizeof(d), cudaMemcpyDeviceToHost), "state");
+  if (c1) *c1 = d.central[0] < 0 ? -1 : d.central[0] - s->off;
+  if (c2) *c2 = d.central[1] < 0 ? -1 : d.central[1] - s->off;
+  if (h1) memcpy(h1, d.halo_c[0], 3 * sizeof(double));
+  if (h2) memcpy(h2, d.halo_c[1], 3 * sizeof(double));
   return GS_OK;
 }
 
 int gs_sort_build(gs_ctx* ctx) {
   CTX_CHECK(ctx);
+  int rc = ensure_layout(ctx);
+  if (rc) return rc;
+  if (!ctx->lay.nseg) return GS_OK;
   enqueue_sort_build(ctx, 0);
   CK(ctx, cudaGetLastError(), "sort/build");
+  for (Slot& s : ctx->slots)
+    if (s.live) s.tree = Slot::kTreeBuilt;
   return GS_OK;
 }
 
@@ -724,6 +1121,9 @@ int gs_set_com_mode(gs_ctx* ctx, int mode) {
 
 int gs_run(gs_ctx* ctx, uint32_t nsteps, int do_sf) {
   CTX_CHECK(ctx);
+  int rc = ensure_layout(ctx);
+  if (rc) return rc;
+  if (!ctx->lay.nseg) return GS_OK;
   for (uint32_t s = 0; s < nsteps; s++) {
     const int key = (ctx->cur) | (ctx->scur << 1) | ((do_sf ? 1 : 0) << 2) | ((ctx->debug ? 1 : 0) << 3);
     auto it = ctx->graphs.find(key);
@@ -737,6 +1137,17 @@ int gs_run(gs_ctx* ctx, uint32_t nsteps, int do_sf) {
       ctx->cur = cur0;
       ctx->scur = scur0;
       CK(ctx, e, "end capture");
+      size_t nn = 0;
+      if (cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess) {
+        std::vector<cudaGraphNode_t> nodes(nn);
+        uint32_t nk = 0;
+        if (nn && cudaGraphGetNodes(g, nodes.data(), &nn) == cudaSuccess)
+          for (cudaGraphNode_t n : nodes) {
+            cudaGraphNodeType t;
+            if (cudaGraphNodeGetType(n, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) nk++;
+          }
+        ctx->step_kernels = nk;
+      }
       cudaGraphExec_t ge = nullptr;
       e = cudaGraphInstantiate(&ge, g, 0);
       cudaGraphDestroy(g);
@@ -746,8 +1157,16 @@ int gs_run(gs_ctx* ctx, uint32_t nsteps, int do_sf) {
     CK(ctx, cudaGraphLaunch(it->second, ctx->stream), "graph launch");
     // a step gathers cur -> cur^1 then walks back: cur unchanged, stellar flipped
     ctx->scur ^= 1;
-    ctx->tree = gs_ctx::kTreeBuilt;
   }
+  for (Slot& s : ctx->slots)
+    if (s.live && nsteps) s.tree = Slot::kTreeBuilt;
+  return GS_OK;
+}
+
+int gs_step_kernels(gs_ctx* ctx, uint32_t* n) {
+  CTX_CHECK(ctx);
+  if (!n) return ctx->fail(GS_EINVAL, "n is NULL");
+  *n = ctx->step_kernels;
   return GS_OK;
 }
 
@@ -760,41 +1179,47 @@ int gs_stream(gs_ctx* ctx, void** stream) {
 
 int gs_sync(gs_ctx* ctx, uint64_t timeout_ns) {
   CTX_CHECK(ctx);
-  return wait_stream(ctx, timeout_ns);
+  return wait_stream(ctx, timeout_ns, nullptr);
 }
 
 int gs_get_tree(gs_ctx* ctx, gs_node* nodes, uint32_t nodes_cap, uint32_t* num_nodes,
                 uint32_t* level_ranges, uint32_t lr_cap, uint32_t* n_levels, uint32_t* perm) {
   CTX_CHECK(ctx);
-  int rc = wait_stream(ctx, 0);
+  SLOT(ctx, s);
+  int rc = wait_stream(ctx, 0, s);
   if (rc) return rc;
-  if (ctx->tree == gs_ctx::kTreeNone) return ctx->fail(GS_ENOTREADY, "no tree yet");
-  if (!ctx->bh) {
-    CK(ctx, ctx->ws.alloc(&ctx->bh, ctx->ws.cap), "bh staging");
-    ctx->max_bh = ctx->ws.cap;
-  }
+  if (s->tree == Slot::kTreeNone) return ctx->fail(GS_ENOTREADY, "no tree yet");
   uint32_t nn = 0, nl = 0;
   std::vector<uint32_t> lr;
-  if (ctx->tree == gs_ctx::kTreeBuilt) {
+  if (s->tree == Slot::kTreeBuilt) {
+    rc = ensure_layout(ctx);
+    if (rc) return rc;
     TreeMeta m;
-    CK(ctx, cudaMemcpy(&m, ctx->ws.meta, sizeof(m), cudaMemcpyDeviceToHost), "meta");
+    CK(ctx, cudaMemcpy(&m, ctx->meta + ctx->sel, sizeof(m), cudaMemcpyDeviceToHost), "meta");
     nn = m.num_nodes;
     nl = m.num_levels;
     for (uint32_t l = 0; l < nl; l++) {
       lr.push_back(m.level_start[l]);
       lr.push_back(m.level_count[l]);
     }
-    if (nodes) {
-      tree_bhnode_kernel<<<grid_for(nn, 256, 148 * 8), 256, 0, ctx->stream>>>(ctx->ws.bb(ctx->ws.cap),
+    if (nodes && nn) {
+      rc = stage_grow(ctx, nn);
+      if (rc) return rc;
+      tree_bhnode_kernel<<<grid_for(nn, 256, 148 * 8), 256, 0, ctx->stream>>>(ctx->bb(), ctx->lay, s->rank,
                                                                                ctx->bh);
       CK(ctx, cudaGetLastError(), "materialise");
     }
   } else {
-    nn = ctx->up_nodes;
-    nl = (uint32_t)ctx->up_lr.size() / 2;
-    lr = ctx->up_lr;
+    nn = s->up_nodes;
+    nl = (uint32_t)s->up_lr.size() / 2;
+    lr = s->up_lr;
     if (nodes && nn) {
-      bh_patch_kernel<<<grid_for(nn, 256, 148 * 8), 256, 0, ctx->stream>>>(ctx->bh, ctx->ws.cm, nn);
+      rc = stage_grow(ctx, nn);
+      if (rc) return rc;
+      CK(ctx, cudaMemcpyAsync(ctx->bh, s->up_host.data(), sizeof(gs_node) * nn, cudaMemcpyHostToDevice,
+                              ctx->stream),
+         "tree");
+      bh_patch_kernel<<<grid_for(nn, 256, 148 * 8), 256, 0, ctx->stream>>>(ctx->bh, ctx->cm + s->node_off, nn);
       CK(ctx, cudaGetLastError(), "patch");
     }
   }
@@ -803,47 +1228,56 @@ int gs_get_tree(gs_ctx* ctx, gs_node* nodes, uint32_t nodes_cap, uint32_t* num_n
   if (level_ranges)
     memcpy(level_ranges, lr.data(), sizeof(uint32_t) * std::min<size_t>(lr.size(), 2 * (size_t)lr_cap));
   if (nodes && nn)
-    CK(ctx, cudaMemcpyAsync(nodes, ctx->bh, sizeof(gs_node) * std::min(nn, nodes_cap),
-                            cudaMemcpyDeviceToHost, ctx->stream),
+    CK(ctx, cudaMemcpyAsync(nodes, ctx->bh, sizeof(gs_node) * std::min(nn, nodes_cap), cudaMemcpyDeviceToHost,
+                            ctx->stream),
        "nodes");
-  if (perm) CK(ctx, cudaMemcpyAsync(perm, ctx->ws.vals[0], sizeof(uint32_t) * ctx->N, cudaMemcpyDeviceToHost, ctx->stream), "perm");
-  return wait_stream(ctx, 0);
+  if (perm)
+    CK(ctx, cudaMemcpyAsync(perm, ctx->vals[0] + s->off, sizeof(uint32_t) * s->n, cudaMemcpyDeviceToHost,
+                            ctx->stream),
+       "perm");
+  rc = wait_stream(ctx, 0, s);
+  if (rc) return rc;
+  if (perm)
+    for (uint32_t i = 0; i < s->n; i++) perm[i] -= s->off;  // galaxy-local indices
+  return GS_OK;
 }
 
 int gs_read_state(gs_ctx* ctx, float* particles8, float* stellar4) {
   CTX_CHECK(ctx);
+  SLOT(ctx, s);
   if (particles8)
-    CK(ctx, cudaMemcpyAsync(particles8, ctx->part[ctx->cur], (size_t)ctx->N * 32,
+    CK(ctx, cudaMemcpyAsync(particles8, ctx->part[ctx->cur] + 2 * (size_t)s->off, (size_t)s->n * 32,
                             cudaMemcpyDeviceToHost, ctx->stream),
        "state");
   if (stellar4)
-    CK(ctx, cudaMemcpyAsync(stellar4, ctx->stel[ctx->scur], (size_t)ctx->N * 16,
-                            cudaMemcpyDeviceToHost, ctx->stream),
+    CK(ctx, cudaMemcpyAsync(stellar4, ctx->stel[ctx->scur] + s->off, (size_t)s->n * 16, cudaMemcpyDeviceToHost,
+                            ctx->stream),
        "stellar");
-  return wait_stream(ctx, 0);
+  return wait_stream(ctx, 0, s);
 }
 
 // Stream-ordered: both ping-pong buffers get the state (like NBodyGPU._init).
 int gs_write_state(gs_ctx* ctx, const float* particles8, const float* stellar4) {
   CTX_CHECK(ctx);
+  SLOT(ctx, s);
   for (int k = 0; k < 2; k++) {
     if (particles8)
-      CK(ctx, cudaMemcpyAsync(ctx->part[k], particles8, (size_t)ctx->N * 32, cudaMemcpyHostToDevice,
-                              ctx->stream),
+      CK(ctx, cudaMemcpyAsync(ctx->part[k] + 2 * (size_t)s->off, particles8, (size_t)s->n * 32,
+                              cudaMemcpyHostToDevice, ctx->stream),
          "state");
     if (stellar4)
-      CK(ctx, cudaMemcpyAsync(ctx->stel[k], stellar4, (size_t)ctx->N * 16, cudaMemcpyHostToDevice,
+      CK(ctx, cudaMemcpyAsync(ctx->stel[k] + s->off, stellar4, (size_t)s->n * 16, cudaMemcpyHostToDevice,
                               ctx->stream),
          "stellar");
   }
-  return wait_stream(ctx, 0);
+  return wait_stream(ctx, 0, s);
 }
 
 int gs_set_debug(gs_ctx* ctx, int enable) {
   CTX_CHECK(ctx);
   if (enable && !ctx->dbg_acc) {
-    CK(ctx, ctx->ws.alloc(&ctx->dbg_acc, ctx->N), "debug acc");
-    CK(ctx, ctx->ws.alloc(&ctx->dbg_dens, ctx->N), "debug density");
+    CK(ctx, ctx->alloc(&ctx->dbg_acc, ctx->plan.cap), "debug acc");
+    CK(ctx, ctx->alloc(&ctx->dbg_dens, ctx->plan.cap), "debug density");
   }
   ctx->debug = enable != 0;
   return GS_OK;
@@ -851,24 +1285,26 @@ int gs_set_debug(gs_ctx* ctx, int enable) {
 
 int gs_read_forces(gs_ctx* ctx, float* acc4, float* density) {
   CTX_CHECK(ctx);
+  SLOT(ctx, s);
   if (!ctx->dbg_acc) return ctx->fail(GS_ENOTREADY, "gs_set_debug(ctx, 1) first");
-  int rc = wait_stream(ctx, 0);
+  int rc = wait_stream(ctx, 0, s);
   if (rc) return rc;
-  if (acc4) CK(ctx, cudaMemcpy(acc4, ctx->dbg_acc, (size_t)ctx->N * 16, cudaMemcpyDeviceToHost), "acc");
+  if (acc4)
+    CK(ctx, cudaMemcpy(acc4, ctx->dbg_acc + s->off, (size_t)s->n * 16, cudaMemcpyDeviceToHost), "acc");
   if (density)
-    CK(ctx, cudaMemcpy(density, ctx->dbg_dens, (size_t)ctx->N * 4, cudaMemcpyDeviceToHost), "dens");
+    CK(ctx, cudaMemcpy(density, ctx->dbg_dens + s->off, (size_t)s->n * 4, cudaMemcpyDeviceToHost), "dens");
   return GS_OK;
 }
 
 int gs_energy(gs_ctx* ctx, gs_diag* out) {
   CTX_CHECK(ctx);
+  SLOT(ctx, s);
   if (!out) return ctx->fail(GS_EINVAL, "out is NULL");
-  diag_reduce_kernel<<<1, dim3(32, kPartials), 0, ctx->stream>>>(ctx->partials, ctx->walk_groups,
-                                                                  ctx->diag_out);
-  CK(ctx, cudaGetLastError(), "diag");
   double h[kPartials];
-  CK(ctx, cudaMemcpyAsync(h, ctx->diag_out, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "diag");
-  int rc = wait_stream(ctx, 0);
+  CK(ctx, cudaMemcpyAsync(h, ctx->diag_out + (size_t)ctx->sel * kPartials, sizeof(h), cudaMemcpyDeviceToHost,
+                          ctx->stream),
+     "diag");
+  int rc = wait_stream(ctx, 0, s);
   if (rc) return rc;
   out->e_diag = h[0];
   out->e_true = h[1];
@@ -881,70 +1317,95 @@ int gs_energy(gs_ctx* ctx, gs_diag* out) {
 
 int gs_device_errors(gs_ctx* ctx, uint32_t* bits, int clear) {
   CTX_CHECK(ctx);
+  SLOT(ctx, s);
+  (void)s;
   CK(ctx, cudaStreamSynchronize(ctx->stream), "sync");
   unsigned e = 0;
-  CK(ctx, cudaMemcpy(&e, &ctx->st->err, 4, cudaMemcpyDeviceToHost), "err");
+  CK(ctx, cudaMemcpy(&e, &ctx->st[ctx->sel].err, 4, cudaMemcpyDeviceToHost), "err");
   if (bits) *bits = e;
-  if (clear) CK(ctx, cudaMemset(&ctx->st->err, 0, 4), "clear");
+  if (clear) CK(ctx, cudaMemset(&ctx->st[ctx->sel].err, 0, 4), "clear");
   return GS_OK;
 }
 
 int gs_counters(gs_ctx* ctx, uint64_t out[3], int reset) {
   CTX_CHECK(ctx);
+  SLOT(ctx, s);
+  (void)s;
   CK(ctx, cudaStreamSynchronize(ctx->stream), "sync");
   unsigned long long c[3];
-  CK(ctx, cudaMemcpy(c, ctx->st->counters, sizeof(c), cudaMemcpyDeviceToHost), "counters");
+  CK(ctx, cudaMemcpy(c, ctx->st[ctx->sel].counters, sizeof(c), cudaMemcpyDeviceToHost), "counters");
   if (out)
     for (int k = 0; k < 3; k++) out[k] = c[k];
-  if (reset) CK(ctx, cudaMemset(ctx->st->counters, 0, sizeof(c)), "reset");
+  if (reset) CK(ctx, cudaMemset(ctx->st[ctx->sel].counters, 0, sizeof(c)), "reset");
   return GS_OK;
 }
+
+}  // extern "C"
 
 // ---- stateless mortonTree.js entry points ----------------------------------------------
 
 namespace {
+
+// A one-galaxy pool of N particles whose buffers the stateless calls fill.
 struct TmpCtx {
-  Workspace w;
-  cudaStream_t s = nullptr;
-  float4* pos = nullptr;
-  DevState* st = nullptr;
-  ~TmpCtx() {
-    if (s) cudaStreamSynchronize(s);
-    w.release();
-    if (s) cudaStreamDestroy(s);
-  }
+  gs_ctx* c = nullptr;
+  ~TmpCtx() { gs_destroy(c); }
 };
 
-int tmp_fail(cudaError_t e, const char* what) {
-  set_err(g_err, "%s: %s", what, cudaGetErrorString(e));
-  return e == cudaErrorMemoryAllocation ? GS_ENOMEM : GS_ECUDA;
-}
-
-#define TK(expr, what)                                \
-  do {                                                \
-    cudaError_t _e = (expr);                          \
-    if (_e != cudaSuccess) return tmp_fail(_e, what); \
-  } while (0)
-
-int tmp_init(TmpCtx& t, uint32_t N) {
-  TK(cudaStreamCreateWithFlags(&t.s, cudaStreamNonBlocking), "stream");
-  TK(t.w.init(N), "workspace");
-  TK(t.w.alloc(&t.pos, N), "positions");
-  TK(t.w.alloc(&t.st, 1), "state");
-  TK(cudaMemset(t.st, 0, sizeof(DevState)), "state");
-  return GS_OK;
+int tmp_init(TmpCtx& t, uint32_t N, uint32_t max_nodes) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int rc = gs_pool_create(dev, N, 1, &t.c);
+  if (rc) return rc;
+  gs_ctx* c = t.c;
+  Slot& s = c->slots[0];
+  s.live = true;
+  s.off = 0;
+  s.n = s.span = N;
+  s.node_off = 0;
+  s.node_cap = 2 * N + 4096;
+  s.max_nodes = max_nodes;
+  c->single = true;
+  DevState st0;
+  memset(&st0, 0, sizeof(st0));
+  st0.central[0] = st0.central[1] = -1;
+  if (cudaMemcpy(c->st, &st0, sizeof(st0), cudaMemcpyHostToDevice) != cudaSuccess) {
+    set_err(g_err, "state upload failed");
+    return GS_ECUDA;
+  }
+  rc = ensure_layout(c);
+  if (rc) set_err(g_err, "%s", c->err);
+  return rc;
 }
 
 int tmp_check(TmpCtx& t) {
-  TK(cudaStreamSynchronize(t.s), "sync");
-  unsigned e = 0;
-  TK(cudaMemcpy(&e, &t.st->err, 4, cudaMemcpyDeviceToHost), "err");
-  if (e) {
-    set_err(g_err, "device error word 0x%x", e);
-    return (e & GS_DERR_NODES) ? GS_EINVAL : GS_EDEVICE;
+  gs_ctx* c = t.c;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_err(g_err, "%s", cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? GS_ENOMEM : GS_ECUDA;
+  }
+  unsigned err = 0;
+  if ((e = cudaMemcpy(&err, &c->st[0].err, 4, cudaMemcpyDeviceToHost)) != cudaSuccess) {
+    set_err(g_err, "%s", cudaGetErrorString(e));
+    return GS_ECUDA;
+  }
+  if (err) {
+    set_err(g_err, "device error word 0x%x", err);
+    return (err & GS_DERR_NODES) ? GS_EINVAL : GS_EDEVICE;
   }
   return GS_OK;
 }
+
+#define TK(expr, what)                                                     \
+  do {                                                                     \
+    cudaError_t _e = (expr);                                               \
+    if (_e != cudaSuccess) {                                               \
+      set_err(g_err, "%s: %s", (what), cudaGetErrorString(_e));            \
+      return _e == cudaErrorMemoryAllocation ? GS_ENOMEM : GS_ECUDA;       \
+    }                                                                      \
+  } while (0)
 
 // The single empty leaf MortonTree.build makes for N = 0.
 void empty_tree(double root, gs_node* nodes, uint32_t* num, uint32_t* lr, uint32_t* nl) {
@@ -966,8 +1427,9 @@ int tree_outputs(TmpCtx& t, uint32_t max_nodes, gs_node* nodes, uint32_t* num_no
                  uint32_t* level_ranges, uint32_t lr_cap, uint32_t* n_levels) {
   int rc = tmp_check(t);
   if (rc) return rc;
+  gs_ctx* c = t.c;
   TreeMeta m;
-  TK(cudaMemcpy(&m, t.w.meta, sizeof(m), cudaMemcpyDeviceToHost), "meta");
+  TK(cudaMemcpy(&m, c->meta, sizeof(m), cudaMemcpyDeviceToHost), "meta");
   if (m.num_nodes > max_nodes) {
     set_err(g_err, "tree needs %u nodes, pool holds %u", m.num_nodes, max_nodes);
     return GS_EINVAL;
@@ -980,24 +1442,33 @@ int tree_outputs(TmpCtx& t, uint32_t max_nodes, gs_node* nodes, uint32_t* num_no
       level_ranges[2 * l + 1] = m.level_count[l];
     }
   if (nodes) {
-    gs_node* d = nullptr;
-    TK(t.w.alloc(&d, std::max<uint32_t>(m.num_nodes, 1)), "nodes");
-    tree_bhnode_kernel<<<grid_for(m.num_nodes, 256, 148 * 8), 256, 0, t.s>>>(t.w.bb(max_nodes), d);
+    if (stage_grow(c, m.num_nodes)) {
+      set_err(g_err, "%s", c->err);
+      return GS_ENOMEM;
+    }
+    tree_bhnode_kernel<<<grid_for(m.num_nodes, 256, 148 * 8), 256, 0, c->stream>>>(c->bb(), c->lay, 0, c->bh);
     TK(cudaGetLastError(), "materialise");
-    TK(cudaMemcpyAsync(nodes, d, sizeof(gs_node) * m.num_nodes, cudaMemcpyDeviceToHost, t.s), "nodes");
-    TK(cudaStreamSynchronize(t.s), "sync");
+    TK(cudaMemcpyAsync(nodes, c->bh, sizeof(gs_node) * m.num_nodes, cudaMemcpyDeviceToHost, c->stream), "nodes");
+    TK(cudaStreamSynchronize(c->stream), "sync");
   }
   return GS_OK;
 }
+
+__global__ void mask30_kernel(uint32_t* keys, uint32_t N) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+    keys[i] &= 0x3fffffffu;
+}
+
 }  // namespace
 
-int gs_morton_codes(const float* pos, uint32_t N, uint32_t stride, uint32_t* codes,
-                    double* root_size) {
+extern "C" {
+
+int gs_morton_codes(const float* pos, uint32_t N, uint32_t stride, uint32_t* codes, double* root_size) {
   if ((!pos && N) || (!codes && N) || stride < 3) {
     set_err(g_err, "bad arguments");
     return GS_EINVAL;
   }
-  if (N > kMaxN) {
+  if (N > kMaxPool) {
     set_err(g_err, "N too large");
     return GS_EINVAL;
   }
@@ -1006,20 +1477,21 @@ int gs_morton_codes(const float* pos, uint32_t N, uint32_t stride, uint32_t* cod
     return GS_OK;
   }
   TmpCtx t;
-  int rc = tmp_init(t, N);
+  int rc = tmp_init(t, N, 2 * N + 4096);
   if (rc) return rc;
+  gs_ctx* c = t.c;
   std::vector<float4> h;
   host_pack4(pos, N, stride, h);
-  TK(cudaMemcpyAsync(t.pos, h.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, t.s), "upload");
-  const uint32_t bb = grid_for(N, kBBoxThreads, kBBoxBlocks);
-  bbox_kernel<<<bb, kBBoxThreads, 0, t.s>>>(t.pos, 1, N, t.w.bbox_partials, t.w.bbox_counter,
-                                            t.w.frame, t.st, 0);
-  codes_kernel<<<grid_for(N, 256, 148 * 8), 256, 0, t.s>>>(t.pos, 1, N, t.w.frame, t.w.keys[0],
-                                                            nullptr, 0);
+  TK(cudaMemcpyAsync(c->part[0], h.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, c->stream), "upload");
+  const Layout& L = c->lay;
+  bbox_kernel<<<L.flag_tiles, kTileThreads, 0, c->stream>>>(c->part[0], 1, L, c->bbox_part, c->seg_ctr,
+                                                            c->frames, c->st, 0);
+  codes_kernel<<<L.flag_tiles, kTileThreads, 0, c->stream>>>(c->part[0], 1, L, c->frames, c->keys[0], nullptr,
+                                                             0);
   TK(cudaGetLastError(), "codes");
   MortonFrame f;
-  TK(cudaMemcpyAsync(codes, t.w.keys[0], sizeof(uint32_t) * N, cudaMemcpyDeviceToHost, t.s), "codes");
-  TK(cudaMemcpyAsync(&f, t.w.frame, sizeof(f), cudaMemcpyDeviceToHost, t.s), "frame");
+  TK(cudaMemcpyAsync(codes, c->keys[0], sizeof(uint32_t) * N, cudaMemcpyDeviceToHost, c->stream), "codes");
+  TK(cudaMemcpyAsync(&f, c->frames, sizeof(f), cudaMemcpyDeviceToHost, c->stream), "frame");
   rc = tmp_check(t);
   if (rc) return rc;
   if (root_size) *root_size = f.size;
@@ -1032,33 +1504,23 @@ int gs_radix_sort_indices(const uint32_t* codes, uint32_t N, uint32_t* perm) {
     return GS_EINVAL;
   }
   if (N == 0) return GS_OK;
-  if (N > kMaxN) {
+  if (N > kMaxPool) {
     set_err(g_err, "N too large");
     return GS_EINVAL;
   }
   TmpCtx t;
-  int rc = tmp_init(t, N);
+  int rc = tmp_init(t, N, 2 * N + 4096);
   if (rc) return rc;
-  Workspace& w = t.w;
-  TK(cudaMemcpyAsync(w.keys[0], codes, sizeof(uint32_t) * N, cudaMemcpyHostToDevice, t.s), "upload");
+  gs_ctx* c = t.c;
+  const Layout& L = c->lay;
+  TK(cudaMemcpyAsync(c->keys[0], codes, sizeof(uint32_t) * N, cudaMemcpyHostToDevice, c->stream), "upload");
   // radixSortIndices orders by the low 30 bits only (3 x 10-bit digits)
-  mask30_kernel<<<grid_for(N, 256, 148 * 8), 256, 0, t.s>>>(w.keys[0], N);
-  cudaMemsetAsync(w.sort_scratch, 0, w.sort_scratch_bytes, t.s);
-  key_hist_kernel<<<grid_for(N, 256, 148 * 8), 256, 0, t.s>>>(w.keys[0], N, w.hist(), kSortPasses);
-  for (int p = 0; p < kSortPasses; p++) {
-    const int src = p & 1, dst = src ^ 1;
-    uint32_t* lb = w.lookback() + (size_t)p * w.tiles * 256;
-    if (p == 0)
-      onesweep_pass<true><<<w.tiles, kSortThreads, 0, t.s>>>(w.keys[src], nullptr, w.keys[dst],
-                                                             w.vals[dst], w.hist() + p * 256, lb,
-                                                             w.tile_ctr() + p, N, 8 * p, t.st);
-    else
-      onesweep_pass<false><<<w.tiles, kSortThreads, 0, t.s>>>(w.keys[src], w.vals[src], w.keys[dst],
-                                                              w.vals[dst], w.hist() + p * 256, lb,
-                                                              w.tile_ctr() + p, N, 8 * p, t.st);
-  }
+  mask30_kernel<<<grid_for(N, 256, 148 * 8), 256, 0, c->stream>>>(c->keys[0], N);
+  TK(cudaMemsetAsync(c->sort_scratch, 0, sizeof(uint32_t) * c->plan.sort_words, c->stream), "clear");
+  key_hist_kernel<<<L.flag_tiles, kTileThreads, 0, c->stream>>>(c->keys[0], L, c->hist(), kSortPasses);
+  enqueue_sort_passes(c, false);
   TK(cudaGetLastError(), "sort");
-  TK(cudaMemcpyAsync(perm, w.vals[0], sizeof(uint32_t) * N, cudaMemcpyDeviceToHost, t.s), "perm");
+  TK(cudaMemcpyAsync(perm, c->vals[0], sizeof(uint32_t) * N, cudaMemcpyDeviceToHost, c->stream), "perm");
   return tmp_check(t);
 }
 
@@ -1069,63 +1531,61 @@ int gs_tree_build(const uint32_t* sorted_codes, const float* pos3, const float* 
     empty_tree(root_size, nodes, num_nodes, level_ranges, n_levels);
     return GS_OK;
   }
-  if (!sorted_codes || !pos3 || !masses || N > kMaxN) {
+  if (!sorted_codes || !pos3 || !masses || N > kMaxPool) {
     set_err(g_err, "bad arguments");
     return GS_EINVAL;
   }
+  if (max_nodes == 0) max_nodes = 2 * N + 4096;
   TmpCtx t;
-  int rc = tmp_init(t, N);
+  int rc = tmp_init(t, N, max_nodes);
   if (rc) return rc;
+  gs_ctx* c = t.c;
   std::vector<float4> h(N);
-  std::vector<uint32_t> c(N);
+  std::vector<uint32_t> k(N);
   for (uint32_t i = 0; i < N; i++) {
     h[i] = make_float4(pos3[3 * (size_t)i], pos3[3 * (size_t)i + 1], pos3[3 * (size_t)i + 2], masses[i]);
-    c[i] = sorted_codes[i] & 0x3fffffffu;
+    k[i] = sorted_codes[i] & 0x3fffffffu;
   }
-  TK(cudaMemcpyAsync(t.pos, h.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, t.s), "upload");
-  TK(cudaMemcpyAsync(t.w.keys[0], c.data(), sizeof(uint32_t) * N, cudaMemcpyHostToDevice, t.s), "codes");
-  if (max_nodes == 0) max_nodes = 2 * N + 4096;
-  enqueue_build(t.w, t.pos, 1, max_nodes, kComJs, root_size, nullptr, t.s, t.st, nullptr);
+  TK(cudaMemcpyAsync(c->part[0], h.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, c->stream), "upload");
+  TK(cudaMemcpyAsync(c->keys[0], k.data(), sizeof(uint32_t) * N, cudaMemcpyHostToDevice, c->stream), "codes");
+  enqueue_build(c, c->part[0], 1, kComJs, root_size, nullptr);
   TK(cudaGetLastError(), "build");
   return tree_outputs(t, max_nodes, nodes, num_nodes, level_ranges, lr_cap, n_levels);
 }
 
-int gs_sort_and_build(const float* particles8, const float* stellar4, uint32_t N,
-                      int64_t track_idx2, float* sorted8, float* sorted_stellar4, uint32_t* perm,
-                      gs_node* nodes, uint32_t max_nodes, uint32_t* num_nodes,
-                      uint32_t* level_ranges, uint32_t lr_cap, uint32_t* n_levels,
-                      int64_t* central_idx, int64_t* central_idx2, float* sorted_mass) {
+int gs_sort_and_build(const float* particles8, const float* stellar4, uint32_t N, int64_t track_idx2,
+                      float* sorted8, float* sorted_stellar4, uint32_t* perm, gs_node* nodes,
+                      uint32_t max_nodes, uint32_t* num_nodes, uint32_t* level_ranges, uint32_t lr_cap,
+                      uint32_t* n_levels, int64_t* central_idx, int64_t* central_idx2, float* sorted_mass) {
   if (N == 0) {
     empty_tree(-INFINITY, nodes, num_nodes, level_ranges, n_levels);
     if (central_idx) *central_idx = 0;
     if (central_idx2) *central_idx2 = -1;
     return GS_OK;
   }
-  if (!particles8 || N > kMaxN) {
+  if (!particles8 || N > kMaxPool) {
     set_err(g_err, "bad arguments");
     return GS_EINVAL;
   }
-  TmpCtx t;
-  int rc = tmp_init(t, N);
-  if (rc) return rc;
-  float4 *P = nullptr, *P2 = nullptr, *S = nullptr, *S2 = nullptr;
-  TK(t.w.alloc(&P, 2 * (size_t)N), "particles");
-  TK(t.w.alloc(&P2, 2 * (size_t)N), "particles");
-  TK(t.w.alloc(&S, N), "stellar");
-  TK(t.w.alloc(&S2, N), "stellar");
-  TK(cudaMemcpyAsync(P, particles8, (size_t)N * 32, cudaMemcpyHostToDevice, t.s), "upload");
-  if (stellar4) TK(cudaMemcpyAsync(S, stellar4, (size_t)N * 16, cudaMemcpyHostToDevice, t.s), "upload");
-  else TK(cudaMemsetAsync(S, 0, (size_t)N * 16, t.s), "memset");
-  enqueue_codes_sort(t.w, P, 2, t.s, t.st, 0);
-  gather_kernel<<<grid_for(N, 256, 148 * 16), 256, 0, t.s>>>(t.w.vals[0], P, P2, S, S2, N, t.st, 0);
   if (max_nodes == 0) max_nodes = 2 * N + 4096;
-  enqueue_build(t.w, P2, 2, max_nodes, kComJs, 0.0, t.w.frame, t.s, t.st, nullptr);
+  TmpCtx t;
+  int rc = tmp_init(t, N, max_nodes);
+  if (rc) return rc;
+  gs_ctx* c = t.c;
+  float4 *P = c->part[0], *P2 = c->part[1], *S = c->stel[0], *S2 = c->stel[1];
+  TK(cudaMemcpyAsync(P, particles8, (size_t)N * 32, cudaMemcpyHostToDevice, c->stream), "upload");
+  if (stellar4) TK(cudaMemcpyAsync(S, stellar4, (size_t)N * 16, cudaMemcpyHostToDevice, c->stream), "upload");
+  else TK(cudaMemsetAsync(S, 0, (size_t)N * 16, c->stream), "memset");
+  enqueue_codes_sort(c, P, 2, 0);
+  enqueue_sort_passes(c, false);
+  gather_kernel<<<c->lay.flag_tiles, kTileThreads, 0, c->stream>>>(c->vals[0], P, P2, S, S2, c->lay, c->st);
+  enqueue_build(c, P2, 2, kComJs, 0.0, c->frames);
   TK(cudaGetLastError(), "sort and build");
   std::vector<uint32_t> hp(N);
-  TK(cudaMemcpyAsync(hp.data(), t.w.vals[0], sizeof(uint32_t) * N, cudaMemcpyDeviceToHost, t.s), "perm");
-  if (sorted8) TK(cudaMemcpyAsync(sorted8, P2, (size_t)N * 32, cudaMemcpyDeviceToHost, t.s), "sorted");
+  TK(cudaMemcpyAsync(hp.data(), c->vals[0], sizeof(uint32_t) * N, cudaMemcpyDeviceToHost, c->stream), "perm");
+  if (sorted8) TK(cudaMemcpyAsync(sorted8, P2, (size_t)N * 32, cudaMemcpyDeviceToHost, c->stream), "sorted");
   if (sorted_stellar4)
-    TK(cudaMemcpyAsync(sorted_stellar4, S2, (size_t)N * 16, cudaMemcpyDeviceToHost, t.s), "stellar");
+    TK(cudaMemcpyAsync(sorted_stellar4, S2, (size_t)N * 16, cudaMemcpyDeviceToHost, c->stream), "stellar");
   rc = tree_outputs(t, max_nodes, nodes, num_nodes, level_ranges, lr_cap, n_levels);
   if (rc) return rc;
   int64_t c1 = 0, c2 = -1;

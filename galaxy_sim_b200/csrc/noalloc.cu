@@ -19,7 +19,7 @@
 //
 // All calls share the one array, and it keeps the contents of the last call.
 // Each call therefore clears the histograms, tile counters and look-back
-// words it relies on before using them. Calls whose work overlaps on the GPU
+// words it relies on, and rewrites its one-galaxy layout, before using them. Calls whose work overlaps on the GPU
 // (two streams, or two host threads) race on that shared array: serialize them.
 #include <cuda_runtime.h>
 
@@ -39,13 +39,17 @@ using namespace gs;
 constexpr uint32_t kNoAllocMaxN = 1u << 20;  // 1,048,576 codes
 constexpr uint32_t kNoAllocTiles = (kNoAllocMaxN + kSortTile - 1) / kSortTile;
 constexpr int kNoAllocPasses = 4;
-// two key buffers + one payload buffer, then histograms | tile counters | look-back
+// two key buffers + one payload buffer, then histograms | tile counters |
+// look-back (cleared per call) | the one-galaxy layout (segment, tile map)
 constexpr size_t kKeyWords = (size_t)kNoAllocMaxN;
 constexpr size_t kHistOff = 3 * kKeyWords;
 constexpr size_t kCtrOff = kHistOff + kNoAllocPasses * 256;
 constexpr size_t kLbOff = kCtrOff + 16;
-constexpr size_t kScratchWords = kLbOff + (size_t)kNoAllocPasses * kNoAllocTiles * 256;
-constexpr size_t kClearBytes = (kScratchWords - kHistOff) * sizeof(uint32_t);
+constexpr size_t kSegOff = kLbOff + (size_t)kNoAllocPasses * kNoAllocTiles * 256;  // 16-byte aligned
+constexpr size_t kMapOff = kSegOff + sizeof(SegDesc) / sizeof(uint32_t);
+constexpr size_t kScratchWords = kMapOff + kNoAllocTiles;
+constexpr size_t kClearBytes = (kSegOff - kHistOff) * sizeof(uint32_t);
+static_assert(kSegOff % 4 == 0 && sizeof(SegDesc) % 16 == 0, "segment descriptor alignment");
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kScratchWords];  // about 13 MiB
 static __device__ DevState g_noalloc_state;                                   // error word
@@ -75,6 +79,27 @@ __global__ void noalloc_mask_hist_kernel(const uint32_t* __restrict__ codes, uin
   __syncthreads();
   for (int k = threadIdx.x; k < kNoAllocPasses * 256; k += blockDim.x)
     if (s_hist[k]) atomicAdd(&hist[k], s_hist[k]);
+}
+
+// The layout of one galaxy of N codes at offset 0: its descriptor and the
+// sort-tile map (every tile belongs to galaxy 0).
+__global__ void noalloc_layout_kernel(SegDesc* seg, uint32_t* map, uint32_t N, uint32_t tiles) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    SegDesc d;
+    d.off = 0;
+    d.n = N;
+    d.node_off = 0;
+    d.node_cap = 0;
+    d.sort_tile0 = 0;
+    d.flag_tile0 = 0;
+    d.group0 = 0;
+    d.max_nodes = 0;
+    d.slot = 0;
+    d.diag_chunk0 = 0;
+    d.pad_[0] = d.pad_[1] = 0;
+    *seg = d;
+  }
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tiles; t += gridDim.x * blockDim.x) map[t] = 0;
 }
 
 int fail(int code, const char* msg) {
@@ -124,13 +149,26 @@ extern "C" int gs_radix_sort_indices_noalloc(const uint32_t* d_codes, uint32_t N
   uint32_t* hist = base + kHistOff;
   uint32_t* ctr = base + kCtrOff;
   uint32_t* lb = base + kLbOff;
+  SegDesc* seg = reinterpret_cast<SegDesc*>(base + kSegOff);
+  uint32_t* map = base + kMapOff;
   const uint32_t tiles = (N + kSortTile - 1) / kSortTile;
   // what must start at zero: histograms, tile counters, look-back words, error word
   if ((e = cudaMemsetAsync(hist, 0, kClearBytes, s)) != cudaSuccess) return cuda_fail(e, "clear");
   if ((e = cudaMemsetAsync(&st->err, 0, sizeof(unsigned), s)) != cudaSuccess)
     return cuda_fail(e, "clear");
   const uint32_t grid = std::min<uint32_t>(148 * 8, (N + 255) / 256);
+  noalloc_layout_kernel<<<1, 256, 0, s>>>(seg, map, N, tiles);
   noalloc_mask_hist_kernel<<<grid, 256, 0, s>>>(d_codes, N, k0, hist);
+  Layout L;
+  L.segs = seg;
+  L.seg_of_sort_tile = map;
+  L.seg_of_flag_tile = nullptr;
+  L.seg_of_group = nullptr;
+  L.nseg = 1;
+  L.sort_tiles = tiles;
+  L.flag_tiles = 0;
+  L.groups = 0;
+  L.diag_chunks = 0;
   // pass 0: k0 -> k1 (payload = index) -> v0; 1: -> k0, d_perm; 2: -> k1, v0; 3: -> k0, d_perm
   uint32_t* kin[kNoAllocPasses] = {k0, k1, k0, k1};
   uint32_t* kout[kNoAllocPasses] = {k1, k0, k1, k0};
@@ -139,11 +177,11 @@ extern "C" int gs_radix_sort_indices_noalloc(const uint32_t* d_codes, uint32_t N
   for (int p = 0; p < kNoAllocPasses; p++) {
     uint32_t* plb = lb + (size_t)p * kNoAllocTiles * 256;
     if (p == 0)
-      onesweep_pass<true><<<tiles, kSortThreads, 0, s>>>(kin[p], nullptr, kout[p], vout[p],
-                                                         hist + p * 256, plb, ctr + p, N, 8 * p, st);
+      onesweep_pass<true, false><<<tiles, kSortThreads, 0, s>>>(kin[p], nullptr, kout[p], vout[p], nullptr,
+                                                                hist, p, plb, ctr + p, L, st);
     else
-      onesweep_pass<false><<<tiles, kSortThreads, 0, s>>>(kin[p], vin[p], kout[p], vout[p],
-                                                          hist + p * 256, plb, ctr + p, N, 8 * p, st);
+      onesweep_pass<false, false><<<tiles, kSortThreads, 0, s>>>(kin[p], vin[p], kout[p], vout[p], nullptr,
+                                                                 hist, p, plb, ctr + p, L, st);
   }
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "sort launch");
   unsigned err = 0;

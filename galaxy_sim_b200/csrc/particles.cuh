@@ -1,8 +1,12 @@
 // Per-particle and per-node kernels around the walk: Morton bbox and codes,
-// the permutation gather (with central tracking and the halo-centre EMA), star
+// the permutation gather, central tracking with the halo-centre EMA, star
 // formation, position compaction, per-level COM refresh, uploaded-tree
 // conversion and the FP64 diagnostics reduction.
+//
+// The per-particle kernels run one 1024-particle tile per block over the tile
+// list of a batch layout; a tile lies inside one galaxy.
 #pragma once
+#include "build.cuh"
 #include "common.cuh"
 #include "morton.cuh"
 #include "sort.cuh"
@@ -10,24 +14,47 @@
 
 namespace gs {
 
-constexpr int kBBoxThreads = 256;
-#ifndef GS_BBOX_BLOCKS
-#define GS_BBOX_BLOCKS 1184
-#endif
-constexpr int kBBoxBlocks = GS_BBOX_BLOCKS;  // blocks of the bbox reduction
+constexpr int kTileThreads = kFlagThreads;  // 256 threads x 4 particles = one build tile
+constexpr int kTilePer = kFlagPer;
+constexpr int kTile = kFlagTile;
 
-// Bounding box over finite particles (mortonTree.js:44-52), float min/max
-// as ordered ints; the last block folds the partials, derives the double frame
-// (:53-54) and, when advance_time is set, stamps Params.time = f32(simTime) and
-// advances simTime by dt (main.js:422, :476).
-__global__ void __launch_bounds__(kBBoxThreads)
-    bbox_kernel(const float4* __restrict__ pos, uint32_t stride, uint32_t N, int* partials,
-                unsigned* counter, MortonFrame* frame, DevState* st, int advance_time) {
-  __shared__ int s_red[kBBoxThreads / 32][6];
+struct TileRange {
+  uint32_t slot;
+  uint32_t beg, end;       // pool particles of this tile
+  uint32_t seg_beg, seg_end;
+  uint32_t lt, ntiles;     // tile index within the galaxy, its tile count
+};
+
+__device__ inline TileRange tile_range(const Layout& L, uint32_t tile) {
+  const SegDesc sd = L.segs[L.seg_of_flag_tile[tile]];
+  TileRange t;
+  t.slot = sd.slot;
+  t.seg_beg = sd.off;
+  t.seg_end = sd.off + sd.n;
+  t.lt = tile - sd.flag_tile0;
+  t.ntiles = (sd.n + kTile - 1) / kTile;
+  t.beg = sd.off + t.lt * kTile;
+  t.end = min(t.beg + kTile, t.seg_end);
+  return t;
+}
+
+// Bounding box over finite particles (mortonTree.js:44-52), per galaxy: each
+// tile reduces float min/max as ordered ints into its partial; the galaxy's
+// last tile folds its partials, derives the double frame (:53-54) and, with
+// advance_time, stamps Params.time = f32(simTime) and advances simTime by dt
+// (main.js:422, :476). seg_ctr[slot] counts finished tiles and self-resets.
+__global__ void __launch_bounds__(kTileThreads)
+    bbox_kernel(const float4* __restrict__ pos, uint32_t stride, Layout L, int* partials,
+                unsigned* seg_ctr, MortonFrame* frames, DevState* st, int advance_time) {
+  __shared__ int s_red[kTileThreads / 32][6];
   __shared__ bool s_last;
+  const TileRange t = tile_range(L, blockIdx.x);
   int mn[3] = {float_to_ordered(INFINITY), float_to_ordered(INFINITY), float_to_ordered(INFINITY)};
   int mx[3] = {float_to_ordered(-INFINITY), float_to_ordered(-INFINITY), float_to_ordered(-INFINITY)};
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+#pragma unroll
+  for (int q = 0; q < kTilePer; q++) {
+    const uint32_t i = t.beg + q * kTileThreads + threadIdx.x;
+    if (i >= t.end) break;
     const float4 p = pos[(size_t)i * stride];
     if (isfinite(p.x) && isfinite(p.y) && isfinite(p.z)) {
       const int e[3] = {float_to_ordered(p.x), float_to_ordered(p.y), float_to_ordered(p.z)};
@@ -52,27 +79,28 @@ __global__ void __launch_bounds__(kBBoxThreads)
   __syncthreads();
   if (threadIdx.x < 6) {
     int v = s_red[0][threadIdx.x];
-    for (int w = 1; w < kBBoxThreads / 32; w++)
+    for (int w = 1; w < kTileThreads / 32; w++)
       v = threadIdx.x < 3 ? min(v, s_red[w][threadIdx.x]) : max(v, s_red[w][threadIdx.x]);
     partials[blockIdx.x * 6 + threadIdx.x] = v;
   }
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  if (threadIdx.x == 0) s_last = atomicAdd(&seg_ctr[t.slot], 1u) == t.ntiles - 1;
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  // fold the per-block partials with the whole block (independent loads in flight)
+  // fold the galaxy's tile partials with the whole block (independent loads in flight)
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     mn[k] = float_to_ordered(INFINITY);
     mx[k] = float_to_ordered(-INFINITY);
   }
-  for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+  const uint32_t t0 = blockIdx.x - t.lt;
+  for (uint32_t b = threadIdx.x; b < t.ntiles; b += blockDim.x) {
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-      mn[k] = min(mn[k], __ldcg(&partials[b * 6 + k]));
-      mx[k] = max(mx[k], __ldcg(&partials[b * 6 + 3 + k]));
+      mn[k] = min(mn[k], __ldcg(&partials[(t0 + b) * 6 + k]));
+      mx[k] = max(mx[k], __ldcg(&partials[(t0 + b) * 6 + 3 + k]));
     }
   }
 #pragma unroll
@@ -89,7 +117,7 @@ __global__ void __launch_bounds__(kBBoxThreads)
   __syncthreads();
   if (threadIdx.x < 6) {
     int v = s_red[0][threadIdx.x];
-    for (int w = 1; w < kBBoxThreads / 32; w++)
+    for (int w = 1; w < kTileThreads / 32; w++)
       v = threadIdx.x < 3 ? min(v, s_red[w][threadIdx.x]) : max(v, s_red[w][threadIdx.x]);
     s_red[0][threadIdx.x] = v;
   }
@@ -100,109 +128,145 @@ __global__ void __launch_bounds__(kBBoxThreads)
       fmn[k] = ordered_to_float(s_red[0][k]);
       fmx[k] = ordered_to_float(s_red[0][3 + k]);
     }
-    *frame = frame_from_bbox(fmn, fmx);
-    *counter = 0;
-    if (advance_time && st) {
-      st->p.time = __double2float_rn(st->sim_time);
-      st->sim_time = __dadd_rn(st->sim_time, (double)st->p.dt);
+    frames[t.slot] = frame_from_bbox(fmn, fmx);
+    seg_ctr[t.slot] = 0;
+    if (advance_time) {
+      DevState* s = st + t.slot;
+      s->p.time = __double2float_rn(s->sim_time);
+      s->sim_time = __dadd_rn(s->sim_time, (double)s->p.dt);
     }
   }
 }
 
-// Codes (mortonTree.js:55-60) + the digit histograms of every sort pass.
-__global__ void __launch_bounds__(256)
-    codes_kernel(const float4* __restrict__ pos, uint32_t stride, uint32_t N,
-                 const MortonFrame* __restrict__ frame, uint32_t* __restrict__ codes,
+// Codes (mortonTree.js:55-60) + the digit histograms of every sort pass, per
+// galaxy (hist: [slots][passes][256]).
+__global__ void __launch_bounds__(kTileThreads)
+    codes_kernel(const float4* __restrict__ pos, uint32_t stride, Layout L,
+                 const MortonFrame* __restrict__ frames, uint32_t* __restrict__ codes,
                  uint32_t* hist, int passes) {
-  __shared__ uint32_t s_hist[4 * 256];
-  for (int k = threadIdx.x; k < 4 * 256; k += blockDim.x) s_hist[k] = 0;
+  __shared__ uint32_t s_hist[kSortPasses * 256];
+  const TileRange t = tile_range(L, blockIdx.x);
+  if (hist)
+    for (int k = threadIdx.x; k < passes * 256; k += blockDim.x) s_hist[k] = 0;
   __syncthreads();
-  const MortonFrame f = *frame;
-  const uint32_t stride_all = gridDim.x * blockDim.x;
-  for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < N; i0 += stride_all) {
-    const uint32_t i = i0 + threadIdx.x;
-    const bool valid = i < N;
+  const MortonFrame f = frames[t.slot];
+#pragma unroll
+  for (int q = 0; q < kTilePer; q++) {
+    const uint32_t i = t.beg + q * kTileThreads + threadIdx.x;
+    const bool valid = i < t.end;
     uint32_t code = 0;
     if (valid) {
       const float4 p = pos[(size_t)i * stride];
       code = morton_code(f, p.x, p.y, p.z);
       codes[i] = code;
     }
-#ifndef GS_HIST_MATCH
     if (hist && valid)
       for (int p = 0; p < passes; p++) atomicAdd(&s_hist[p * 256 + ((code >> (8 * p)) & 255u)], 1u);
-#else
-    if (hist) hist_add_warp(s_hist, code, valid, passes);
-#endif
   }
   if (!hist) return;
   __syncthreads();
+  uint32_t* h = hist + (size_t)t.slot * kSortPasses * 256;
   for (int k = threadIdx.x; k < passes * 256; k += blockDim.x)
-    if (s_hist[k]) atomicAdd(&hist[k], s_hist[k]);
+    if (s_hist[k]) atomicAdd(&h[k], s_hist[k]);
+}
+
+// Digit histograms of given keys (stateless sort entry points).
+__global__ void __launch_bounds__(kTileThreads)
+    key_hist_kernel(const uint32_t* __restrict__ keys, Layout L, uint32_t* hist, int passes) {
+  __shared__ uint32_t s_hist[kSortPasses * 256];
+  const TileRange t = tile_range(L, blockIdx.x);
+  for (int k = threadIdx.x; k < passes * 256; k += blockDim.x) s_hist[k] = 0;
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < kTilePer; q++) {
+    const uint32_t i = t.beg + q * kTileThreads + threadIdx.x;
+    const bool valid = i < t.end;
+    hist_add_warp(s_hist, valid ? keys[i] : 0u, valid, passes);
+  }
+  __syncthreads();
+  uint32_t* h = hist + (size_t)t.slot * kSortPasses * 256;
+  for (int k = threadIdx.x; k < passes * 256; k += blockDim.x)
+    if (s_hist[k]) atomicAdd(&h[k], s_hist[k]);
 }
 
 // Gather dst[i] = src[perm[i]] of the 32-byte particle and 16-byte stellar
-// records (nbody_bh.wgsl:322-326, :336-340). With tracking, the thread whose
-// source is a tracked central particle records its new index
-// (bhWorker.js:67-68) and moves that halo centre 10% of the way to the particle
-// (main.js:449-457, in double like the JS numbers), then stores the f32 copy
-// in Params (NBodyGPU.js:272-273).
-__global__ void __launch_bounds__(256)
+// records (nbody_bh.wgsl:322-326, :336-340). perm holds pool indices of the
+// same galaxy; anything else is flagged, never dereferenced.
+__global__ void __launch_bounds__(kTileThreads)
     gather_kernel(const uint32_t* __restrict__ perm, const float4* __restrict__ pin,
                   float4* __restrict__ pout, const float4* __restrict__ sin,
-                  float4* __restrict__ sout, uint32_t N, DevState* st, int track) {
-  long long c0 = -1, c1 = -1;
-  if (track) {
-    c0 = st->central[0];
-    c1 = st->central[1];
-  }
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+                  float4* __restrict__ sout, Layout L, DevState* st) {
+  const TileRange t = tile_range(L, blockIdx.x);
+#pragma unroll
+  for (int q = 0; q < kTilePer; q++) {
+    const uint32_t i = t.beg + q * kTileThreads + threadIdx.x;
+    if (i >= t.end) break;
     const uint32_t s = perm[i];
-    if (s >= N) {  // a corrupted permutation is flagged, never dereferenced
-      raise_err(st, GS_DERR_LOOKBACK);
+    if (s < t.seg_beg || s >= t.seg_end) {
+      raise_err(st + t.slot, GS_DERR_LOOKBACK);
       continue;
     }
     const float4 a = pin[2 * (size_t)s], b = pin[2 * (size_t)s + 1];
     pout[2 * (size_t)i] = a;
     pout[2 * (size_t)i + 1] = b;
     if (sout) sout[i] = sin[s];
-    if (track) {
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const long long c = h == 0 ? c0 : c1;
-        if (c >= 0 && (long long)s == c) {
-          st->central_next[h] = i;
-          if (h < (int)st->p.haloCount) {
-            const float q[3] = {a.x, a.y, a.z};
-            float* dst = h == 0 ? st->p.haloC1 : st->p.haloC2;
-            for (int k = 0; k < 3; k++) {
-              const double hc = st->halo_c[h][k];
-              const double nv = __dadd_rn(hc, __dmul_rn(__dsub_rn((double)q[k], hc), 0.1));
-              st->halo_c[h][k] = nv;
-              dst[k] = __double2float_rn(nv);
-            }
-          }
-        }
+  }
+}
+
+// Central-particle tracking after a sort (one thread per galaxy): the tracked
+// index follows the permutation (bhWorker.js:67-68) through inv[old] = new, and
+// the halo centre moves 10% of the way to the particle (main.js:449-457, in
+// double like the JS numbers); its f32 copy goes to Params (NBodyGPU.js:272-273).
+__global__ void track_kernel(const uint32_t* __restrict__ inv, const float4* __restrict__ P,
+                             Layout L, DevState* st) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= L.nseg) return;
+  const SegDesc sd = L.segs[r];
+  DevState* s = st + sd.slot;
+  for (int h = 0; h < 2; h++) {
+    const long long c = s->central[h];
+    if (c < (long long)sd.off || c >= (long long)sd.off + sd.n) continue;  // -1: not tracked
+    const uint32_t ni = inv[c];
+    if (ni < sd.off || ni >= sd.off + sd.n) {
+      raise_err(s, GS_DERR_LOOKBACK);
+      continue;
+    }
+    s->central[h] = ni;
+    if (h < (int)s->p.haloCount) {
+      const float4 a = P[2 * (size_t)ni];
+      const float q[3] = {a.x, a.y, a.z};
+      float* dst = h == 0 ? s->p.haloC1 : s->p.haloC2;
+      for (int k = 0; k < 3; k++) {
+        const double hc = s->halo_c[h][k];
+        const double nv = __dadd_rn(hc, __dmul_rn(__dsub_rn((double)q[k], hc), 0.1));
+        s->halo_c[h][k] = nv;
+        dst[k] = __double2float_rn(nv);
       }
     }
   }
 }
 
-// star_formation as its own pass (NBodyGPU.encodeStarFormation).
-__global__ void sf_kernel(float4* __restrict__ P, float4* __restrict__ S, uint32_t N,
-                          const DevState* __restrict__ st) {
-  const gs_params prm = st->p;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+// star_formation as its own pass (NBodyGPU.encodeStarFormation); the RNG
+// stream index is the particle's index within its galaxy.
+__global__ void __launch_bounds__(kTileThreads)
+    sf_kernel(float4* __restrict__ P, float4* __restrict__ S, Layout L,
+              const DevState* __restrict__ st) {
+  const TileRange t = tile_range(L, blockIdx.x);
+  const gs_params prm = st[t.slot].p;
+#pragma unroll
+  for (int q = 0; q < kTilePer; q++) {
+    const uint32_t i = t.beg + q * kTileThreads + threadIdx.x;
+    if (i >= t.end) break;
     float4 p1 = P[2 * (size_t)i + 1];
     float4 s = S[i];
     const float4 p1o = p1, so = s;
-    star_formation_one(prm, i, p1, s);
+    star_formation_one(prm, i - t.seg_beg, p1, s);
     if (p1.x != p1o.x || p1.y != p1o.y || p1.z != p1o.z || p1.w != p1o.w) P[2 * (size_t)i + 1] = p1;
     if (s.x != so.x || s.y != so.y || s.z != so.z || s.w != so.w) S[i] = s;
   }
 }
 
-// compact_positions (nbody_bh.wgsl:188-195).
+// compact_positions (nbody_bh.wgsl:188-195) over one particle range.
 __global__ void compact_kernel(const float4* __restrict__ P, const float* __restrict__ energy,
                                float4* __restrict__ out, uint32_t N) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
@@ -211,7 +275,8 @@ __global__ void compact_kernel(const float4* __restrict__ P, const float* __rest
   }
 }
 
-// refresh_level (nbody_bh.wgsl:288-313) on one BFS level of the walk layout.
+// refresh_level (nbody_bh.wgsl:288-313) on one BFS level of the walk layout
+// (pool indices).
 __global__ void refresh_level_kernel(const float4* __restrict__ P, float4* cm,
                                      const WalkInfo* __restrict__ info, uint32_t start,
                                      uint32_t count) {
@@ -241,23 +306,25 @@ __global__ void refresh_level_kernel(const float4* __restrict__ P, float4* cm,
   cm[n] = m > 0.0f ? make_float4(cx / m, cy / m, cz / m, m) : make_float4(0.f, 0.f, 0.f, m);
 }
 
-// uploadBHTree: BHNode (64 B) -> walk layout. Children of an internal node must
+// uploadBHTree: BHNode (64 B) -> walk layout of one galaxy, whose nodes start at
+// node_off and particles at off of the pools. Children of an internal node must
 // be the contiguous increasing run the BFS build produces (mortonTree.js:146-155).
 // A node that breaks the rules (children not after their parent, ranges past
 // the node or particle arrays) is flagged and made an empty leaf, so a walk
 // over an uploaded tree always terminates and stays in bounds.
 __global__ void upload_convert_kernel(const gs_node* __restrict__ nodes, uint32_t num_nodes,
-                                      uint32_t N, float4* cm, WalkInfo* info, DevState* st) {
+                                      uint32_t N, uint32_t node_off, uint32_t off, float4* cm,
+                                      WalkInfo* info, DevState* st) {
   for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < num_nodes; n += gridDim.x * blockDim.x) {
     const gs_node nd = nodes[n];
-    cm[n] = make_float4(nd.com[0], nd.com[1], nd.com[2], nd.mass);
+    float4 c = make_float4(nd.com[0], nd.com[1], nd.com[2], nd.mass);
     WalkInfo w;
     w.s2 = nd.size * nd.size;
     w.size = nd.size;
     bool ok = true;
     if (nd.isLeaf == 1u) {
       ok = nd.count < kLeafBit && (uint64_t)nd.first + nd.count <= N;
-      w.child = nd.first;
+      w.child = off + nd.first;
       w.info = kLeafBit | (nd.count & ~kLeafBit);
     } else {
       int32_t first = -1;
@@ -270,28 +337,83 @@ __global__ void upload_convert_kernel(const gs_node* __restrict__ nodes, uint32_
         if ((uint32_t)ch >= num_nodes || (uint32_t)ch <= n) ok = false;
         nc++;
       }
-      w.child = first < 0 ? 0u : (uint32_t)first;
+      w.child = node_off + (first < 0 ? 0u : (uint32_t)first);
       w.info = nc;
     }
     if (!ok) {
       raise_err(st, GS_DERR_TREE);
-      w.child = 0;
+      w.child = off;
       w.info = kLeafBit;  // empty leaf
-      cm[n].w = 0.0f;
+      c.w = 0.0f;
     }
-    info[n] = w;
+    cm[node_off + n] = c;
+    info[node_off + n] = w;
   }
 }
 
-// FP64 diagnostics: fold the walk's per-block partials.
-__global__ void diag_reduce_kernel(const double* __restrict__ partials, uint32_t nblocks,
-                                   double* out) {
+// FP64 diagnostics: fold each galaxy's per-group walk partials into
+// out[slot][kPartials]. A block of 32 x kPartials threads sums kDiagChunk groups
+// of one galaxy (chunks counted from the galaxy's first group); the galaxy's
+// last block adds the chunk sums in chunk order, so the result does not depend
+// on the layout or on block timing. diag_ctr[slot] self-resets.
+constexpr uint32_t kDiagChunk = 512;
+__global__ void __launch_bounds__(32 * kPartials)
+    diag_reduce_kernel(const double* __restrict__ partials, Layout L, double* chunk_part,
+                       unsigned* diag_ctr, double* out) {
+  __shared__ bool s_last;
+  const uint32_t x = blockIdx.x;
+  uint32_t lo = 0, hi = L.nseg;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (L.segs[mid].diag_chunk0 <= x) lo = mid;
+    else hi = mid;
+  }
+  const SegDesc sd = L.segs[lo];
+  const uint32_t ng = (sd.n + kWalkGroup - 1) / kWalkGroup;
+  const uint32_t nch = (ng + kDiagChunk - 1) / kDiagChunk;
+  const uint32_t g0 = (x - sd.diag_chunk0) * kDiagChunk, g1 = min(ng, g0 + kDiagChunk);
   const int k = threadIdx.y, lane = threadIdx.x;
   double v = 0;
-  for (uint32_t b = lane; b < nblocks; b += 32) v += partials[(size_t)b * kPartials + k];
+  for (uint32_t b = g0 + lane; b < g1; b += 32) v += partials[(size_t)(sd.group0 + b) * kPartials + k];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if (lane == 0) out[k] = v;
+  if (lane == 0) chunk_part[(size_t)x * kPartials + k] = v;
+  __threadfence();
+  __syncthreads();
+  if (lane == 0 && k == 0) s_last = atomicAdd(&diag_ctr[sd.slot], 1u) == nch - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double w = 0;
+  for (uint32_t c = lane; c < nch; c += 32) w += __ldcg(&chunk_part[(size_t)(sd.diag_chunk0 + c) * kPartials + k]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+  if (lane == 0) out[(size_t)sd.slot * kPartials + k] = w;
+  if (lane == 0 && k == 0) diag_ctr[sd.slot] = 0;
+}
+
+// Tile / group -> galaxy maps of a layout (binary search over the galaxies'
+// first tiles, which increase with the rank).
+__global__ void layout_maps_kernel(const SegDesc* __restrict__ segs, uint32_t nseg,
+                                   uint32_t* sort_map, uint32_t sort_tiles, uint32_t* flag_map,
+                                   uint32_t flag_tiles, uint32_t* group_map, uint32_t groups) {
+  const uint32_t total = max(sort_tiles, max(flag_tiles, groups));
+  for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < total; x += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int which = 0; which < 3; which++) {
+      const uint32_t lim = which == 0 ? sort_tiles : which == 1 ? flag_tiles : groups;
+      if (x >= lim) continue;
+      uint32_t lo = 0, hi = nseg;
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint32_t f = which == 0 ? segs[mid].sort_tile0
+                                      : which == 1 ? segs[mid].flag_tile0 : segs[mid].group0;
+        if (f <= x) lo = mid;
+        else hi = mid;
+      }
+      (which == 0 ? sort_map : which == 1 ? flag_map : group_map)[x] = lo;
+    }
+  }
 }
 
 }  // namespace gs

@@ -1,8 +1,13 @@
 // Stable LSD radix sort of 32-bit keys with a 32-bit payload, one kernel per
 // 8-bit digit ("onesweep": per-tile ranking by warp match, decoupled look-back
-// for the tile's global digit offsets, direct scatter). A stable sort of
+// for the tile's digit offsets, direct scatter). A stable sort of
 // (code, original index) gives exactly the permutation of radixSortIndices
 // (src/physics/mortonTree.js:68-84): ties keep their original order.
+//
+// Segmented: every galaxy of a batch is sorted within its own particle range
+// by the same four launches. Tiles never cross a galaxy, a galaxy's digit
+// offsets start at its first particle, and the look-back stops at its first
+// tile, so each galaxy's permutation equals the one a solo sort gives.
 #pragma once
 #include "common.cuh"
 
@@ -14,7 +19,8 @@ constexpr int kSortWarps = kSortThreads / 32;
 #define GS_SORT_ITEMS 16
 #endif
 constexpr int kSortItems = GS_SORT_ITEMS;
-constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
+constexpr int kSortTile = kSortThreads * kSortItems;  // keys per tile
+constexpr int kSortPasses = 4;                        // 30-bit codes, 8-bit digits
 constexpr uint32_t kLbAgg = 1u << 30;
 constexpr uint32_t kLbInc = 2u << 30;
 constexpr uint32_t kLbMask = (1u << 30) - 1;
@@ -38,29 +44,40 @@ __device__ inline void hist_add_warp(uint32_t* s_hist, uint32_t key, bool valid,
   }
 }
 
-// One digit pass. FIRST: payload = source index. keys_out may alias nothing.
-template <bool FIRST>
+// One digit pass over every galaxy of the layout. FIRST: payload = source index.
+// LAST: also writes the inverse permutation inv[payload] = destination when
+// inv_out is given (central-particle tracking).
+// hist: [slots][kSortPasses][256] digit counts of each galaxy; lookback: [sort tiles][256];
+// st: per-slot states (error word).
+template <bool FIRST, bool LAST>
 __global__ void __launch_bounds__(kSortThreads)
     onesweep_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                   uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
-                  const uint32_t* __restrict__ hist, uint32_t* lookback, uint32_t* tile_counter,
-                  uint32_t N, int shift, DevState* st) {
+                  uint32_t* __restrict__ inv_out, const uint32_t* __restrict__ hist, int pass,
+                  uint32_t* lookback, uint32_t* tile_counter, Layout L, DevState* st) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kSortWarps][256];
   __shared__ uint32_t s_prefix[256];
   __shared__ uint32_t s_scan[kSortWarps];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int shift = 8 * pass;
   if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
   for (int i = tid; i < kSortWarps * 256; i += kSortThreads) (&s_warp[0][0])[i] = 0;
   __syncthreads();
   const uint32_t tile = s_tile;
-  const uint32_t base = tile * kSortTile + warp * (kSortTile / kSortWarps);
+  if (tile >= L.sort_tiles) return;  // the grid is sized to the tile count
+  const uint32_t seg = L.seg_of_sort_tile[tile];
+  const SegDesc sd = L.segs[seg];
+  DevState* sst = st + sd.slot;
+  const uint32_t lt = tile - sd.sort_tile0;  // tile index within the galaxy
+  const uint32_t seg_end = sd.off + sd.n;
+  const uint32_t base = sd.off + lt * kSortTile + warp * (kSortTile / kSortWarps);
 
   uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
 #pragma unroll
   for (int k = 0; k < kSortItems; k++) {
     const uint32_t idx = base + k * 32 + lane;
-    if (idx < N) {
+    if (idx < seg_end) {
       key[k] = keys_in[idx];
       val[k] = FIRST ? idx : vals_in[idx];
     } else {
@@ -68,14 +85,14 @@ __global__ void __launch_bounds__(kSortThreads)
       val[k] = 0;
     }
   }
-  const unsigned lt = (1u << lane) - 1u;
+  const unsigned lt_mask = (1u << lane) - 1u;
 #pragma unroll
   for (int k = 0; k < kSortItems; k++) {
-    const bool valid = base + k * 32 + lane < N;
+    const bool valid = base + k * 32 + lane < seg_end;
     const uint32_t d = (key[k] >> shift) & 255u;
     const unsigned peers = __match_any_sync(0xffffffffu, valid ? d : 0x100u + lane);
     const uint32_t before = valid ? s_warp[warp][d] : 0u;
-    rank[k] = before + __popc(peers & lt);
+    rank[k] = before + __popc(peers & lt_mask);
     __syncwarp();
     if (valid && (__ffs(peers) - 1) == lane) s_warp[warp][d] = before + __popc(peers);
     __syncwarp();
@@ -91,8 +108,8 @@ __global__ void __launch_bounds__(kSortThreads)
     s_warp[w][d] = tot;
     tot += c;
   }
-  // Global exclusive offset of digit d (block-wide exclusive scan of hist).
-  const uint32_t h = hist[d];
+  // The galaxy's exclusive offset of digit d (block-wide scan of its histogram).
+  const uint32_t h = hist[((size_t)sd.slot * kSortPasses + pass) * 256 + d];
   uint32_t incl = h;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -103,17 +120,17 @@ __global__ void __launch_bounds__(kSortThreads)
   __syncthreads();
   uint32_t wpre = 0;
   for (int w = 0; w < warp; w++) wpre += s_scan[w];
-  const uint32_t gexcl = wpre + incl - h;
+  const uint32_t gexcl = sd.off + wpre + incl - h;
 
   uint32_t* lb = lookback + (size_t)tile * 256;
   uint32_t excl;
-  if (tile == 0) {
+  if (lt == 0) {
     excl = gexcl;
     st_relaxed(&lb[d], kLbInc | (gexcl + tot));
   } else {
     st_relaxed(&lb[d], kLbAgg | tot);
     excl = 0;
-    int64_t t = (int64_t)tile - 1;
+    int64_t t = (int64_t)lt - 1;  // predecessors within the galaxy
     uint32_t spins = 0;
     bool done = false;
     while (t >= 0 && !done) {
@@ -122,7 +139,8 @@ __global__ void __launch_bounds__(kSortThreads)
       uint32_t v[kWin];
 #pragma unroll
       for (int k = 0; k < kWin; k++)
-        v[k] = (t - k >= 0) ? ld_relaxed(lookback + (size_t)(t - k) * 256 + d) : kLbInc;
+        v[k] = (t - k >= 0) ? ld_relaxed(lookback + (size_t)(sd.sort_tile0 + t - k) * 256 + d)
+                            : kLbInc;
       int used = 0;
 #pragma unroll
       for (int k = 0; k < kWin; k++) {
@@ -138,7 +156,7 @@ __global__ void __launch_bounds__(kSortThreads)
       }
       t -= used;
       if (!done && used == 0 && ++spins > kSpinLimit) {
-        raise_err(st, GS_DERR_LOOKBACK);
+        raise_err(sst, GS_DERR_LOOKBACK);
         break;
       }
     }
@@ -149,15 +167,16 @@ __global__ void __launch_bounds__(kSortThreads)
 
 #pragma unroll
   for (int k = 0; k < kSortItems; k++) {
-    if (base + k * 32 + lane < N) {
+    if (base + k * 32 + lane < seg_end) {
       const uint32_t dd = (key[k] >> shift) & 255u;
       const uint32_t pos = s_prefix[dd] + s_warp[warp][dd] + rank[k];
-      if (pos >= N) {  // only after a failed look-back: flag, never write out of bounds
-        raise_err(st, GS_DERR_LOOKBACK);
+      if (pos < sd.off || pos >= seg_end) {  // only after a failed look-back: flag, never write
+        raise_err(sst, GS_DERR_LOOKBACK);
         continue;
       }
       keys_out[pos] = key[k];
       vals_out[pos] = val[k];
+      if (LAST && inv_out) inv_out[val[k]] = pos;
     }
   }
 }

@@ -21,6 +21,8 @@
 //   * Warps are persistent and take 32-particle groups from an atomic counter
 //     (load balance across the dense core); per-group FP64 partials of the
 //     diagnostics replace a block-wide barrier.
+//   * Over a batch, every group belongs to one galaxy and walks that galaxy's
+//     tree with its own Params; warps steal groups across all galaxies.
 #pragma once
 #include "common.cuh"
 
@@ -33,11 +35,7 @@ constexpr int kWalkStack = 96;  // ranges; a range push per opened node, <= 7 * 
 #ifndef GS_WALK_BLOCKS_PER_SM
 #define GS_WALK_BLOCKS_PER_SM 8
 #endif
-#ifndef GS_WALK_CHUNK
-#define GS_WALK_CHUNK 1
-#endif
 constexpr int kWalkBlocksPerSM = GS_WALK_BLOCKS_PER_SM;
-constexpr uint32_t kWalkChunk = GS_WALK_CHUNK;  // consecutive groups per grab: L1 reuse
 constexpr uint32_t kWalkGroup = 32;             // particles per warp (one per lane)
 
 // nbody_bh.wgsl:206-213
@@ -100,14 +98,14 @@ struct WalkArgs {
   float4* __restrict__ stellar;     // in place, used when SF is fused
   const float4* __restrict__ cm;    // node com.xyz, mass
   const WalkInfo* __restrict__ info;
-  DevState* st;
+  DevState* st;                     // per-slot states
   float* __restrict__ energy;       // e_i
   float4* __restrict__ dbg_acc;     // optional {ax, ay, az, phi} (G applied)
   float* __restrict__ dbg_dens;
   double* __restrict__ partials;    // [groups][kPartials]
   unsigned* work;                   // [0] next group, [1] finished warps (self-resetting)
-  uint32_t N;
-  uint32_t node_cap;                // allocated nodes: child ranges must stay below it
+  Layout L;                         // galaxies and the group -> galaxy map
+  SegDesc seg0;                     // the only galaxy, for the one-galaxy instantiation
 };
 
 // Per-warp shared staging.
@@ -183,33 +181,34 @@ __device__ inline void prefetch_l1(const void* p) {
   asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
-template <bool SF, bool DBG>
+// ONE: the layout holds a single galaxy, whose descriptor comes with the
+// kernel parameters instead of a per-group lookup.
+template <bool SF, bool DBG, bool ONE>
 __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(WalkArgs a) {
   __shared__ WalkSmem smem_all[kWalkWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   WalkSmem& S = smem_all[warp];
-  const gs_params& P = a.st->p;  // read-only during the walk; fields loaded where used
-  const float eps2 = __ldg(&P.epsilon2);
-  const float theta2 = __ldg(&P.theta) * __ldg(&P.theta);
-  const float qe2 = 0.25f * eps2;
-  const bool soft = eps2 > 0.0f;  // self pairs may then be summed and removed afterwards
-  const uint32_t ngroups = (a.N + 31) / 32;
+  const uint32_t ngroups = a.L.groups;
   const unsigned full = 0xffffffffu;
 
-  uint32_t g = 0, gstop = 0;
   while (true) {
-    if (g == gstop) {  // grab the next chunk of consecutive groups
-      uint32_t c = 0;
-      if (lane == 0) c = atomicAdd(&a.work[0], 1u);
-      c = __shfl_sync(full, c, 0);
-      g = c * kWalkChunk;
-      gstop = min(g + kWalkChunk, ngroups);
-      if (g >= ngroups) break;
-    }
-    const uint32_t gcur = g++;
-    const uint32_t gbeg = gcur * 32, gend = gbeg + 32;
+    uint32_t c = 0;  // grab the next group of the schedule
+    if (lane == 0) c = atomicAdd(&a.work[0], 1u);
+    c = __shfl_sync(full, c, 0);
+    if (c >= ngroups) break;
+    const uint32_t gcur = c;
+    const SegDesc sd = ONE ? a.seg0 : a.L.segs[a.L.seg_of_group[gcur]];
+    DevState* const sst = a.st + sd.slot;
+    const gs_params& P = sst->p;  // read-only during the walk; fields loaded where used
+    const float eps2 = __ldg(&P.epsilon2);
+    const float theta2 = __ldg(&P.theta) * __ldg(&P.theta);
+    const float qe2 = 0.25f * eps2;
+    const bool soft = eps2 > 0.0f;  // self pairs may then be summed and removed afterwards
+    const uint32_t seg_end = sd.off + sd.n;
+    const uint32_t node_end = sd.node_off + sd.node_cap;
+    const uint32_t gbeg = sd.off + (gcur - sd.group0) * kWalkGroup, gend = gbeg + kWalkGroup;
     const uint32_t i = gbeg + lane;
-    const bool valid = i < a.N;
+    const bool valid = i < seg_end;
     float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0;
     if (valid) {
       p0 = a.pin[2 * (size_t)i];
@@ -222,9 +221,9 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
     const unsigned all = __ballot_sync(full, valid);
 
     int sp = 0;
-    if (lane == 0) S.stack[0] = make_uint2(0u, all);  // the root: range {0, 1}
+    if (lane == 0) S.stack[0] = make_uint2(sd.node_off, all);  // the root: range {node_off, 1}
     sp = 1;
-    uint32_t budget = 4u * a.node_cap + 1024u;
+    uint32_t budget = 4u * sd.node_cap + 1024u;
     while (sp > 0) {
       __syncwarp();
       const uint2 e = S.stack[--sp];
@@ -232,7 +231,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
       const uint32_t cnt = (e.x >> 29) + 1u;
       const unsigned mask = e.y;
       if (--budget == 0) {
-        if (lane == 0) raise_err(a.st, GS_DERR_STACK);
+        if (lane == 0) raise_err(sst, GS_DERR_STACK);
         break;
       }
       __syncwarp();
@@ -324,12 +323,12 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
         const unsigned open = __ballot_sync(full, (obits >> cc) & 1u);
         const uint4 mt = S.cmeta[cc];
         const uint32_t cchild = mt.x, ccnt = mt.y & ~kLeafBit;
-        if (!(cchild > start + cc && (uint64_t)cchild + ccnt <= a.node_cap && ccnt >= 1u && ccnt <= 8u)) {
-          if (lane == 0) raise_err(a.st, GS_DERR_TREE);
+        if (!(cchild > start + cc && (uint64_t)cchild + ccnt <= node_end && ccnt >= 1u && ccnt <= 8u)) {
+          if (lane == 0) raise_err(sst, GS_DERR_TREE);
           continue;
         }
         if (sp >= kWalkStack) {  // cannot happen for depth <= 10 trees
-          if (lane == 0) raise_err(a.st, GS_DERR_STACK);
+          if (lane == 0) raise_err(sst, GS_DERR_STACK);
           continue;
         }
         if (lane == 0) S.stack[sp] = make_uint2(cchild | ((ccnt - 1u) << 29), open);
@@ -346,8 +345,8 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
         const uint32_t cc = __ffs(bb) - 1;
         const uint4 mt = S.cmeta[cc];
         const uint32_t ccnt = mt.y & ~kLeafBit;
-        if ((uint64_t)mt.x + ccnt > a.N) {
-          if (lane == 0) raise_err(a.st, GS_DERR_TREE);
+        if (mt.x < sd.off || (uint64_t)mt.x + ccnt > seg_end) {
+          if (lane == 0) raise_err(sst, GS_DERR_TREE);
           continue;
         }
         if (ccnt > 16u) big |= 1u << cc;
@@ -460,7 +459,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
       if (SF) {
         float4 s = a.stellar[i];
         const float4 s_old = s;
-        star_formation_one(P, i, o1, s);
+        star_formation_one(P, i - sd.off, o1, s);
         if (s.x != s_old.x || s.y != s_old.y || s.z != s_old.z || s.w != s_old.w) a.stellar[i] = s;
       }
       a.pout[2 * (size_t)i] = o0;
@@ -488,9 +487,9 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
         nvisit += __shfl_xor_sync(full, nvisit, o);
       }
       if (lane == 0) {
-        atomicAdd(&a.st->counters[0], nmono);
-        atomicAdd(&a.st->counters[1], npair);
-        atomicAdd(&a.st->counters[2], nvisit);
+        atomicAdd(&sst->counters[0], nmono);
+        atomicAdd(&sst->counters[1], npair);
+        atomicAdd(&sst->counters[2], nvisit);
       }
     }
   }

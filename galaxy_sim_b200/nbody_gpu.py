@@ -20,6 +20,25 @@ import numpy as np
 from ._lib import NODE_DTYPE, GsDiag, GsParams, check, f32, lib, ptr, u32
 
 
+def build_params(N, *, dt, G, epsilon, theta=0.5, haloMass=0, haloA=1, gasDrag=0, time=0,
+                 agingRate=25, sfDensity=1e9, sfEff=0, sfDt=0, haloCenters=()) -> GsParams:
+    """The Params uniform NBodyGPU.updateParams writes (NBodyGPU.js:253-275):
+    epsilon^2 in f32, N forced, at most two halo centres."""
+    p = GsParams()
+    p.dt, p.G = dt, G
+    p.epsilon2 = float(np.float32(epsilon) * np.float32(epsilon))
+    p.N = int(N)
+    p.theta, p.haloMass, p.haloA, p.gasDrag = theta, haloMass, haloA, gasDrag
+    p.time, p.agingRate, p.sfDensity, p.sfEff, p.sfDt = time, agingRate, sfDensity, sfEff, sfDt
+    hc = list(haloCenters or [])
+    p.haloCount = min(len(hc), 2)
+    for h, c in enumerate(hc[:2]):
+        arr = p.haloC1 if h == 0 else p.haloC2
+        for k in range(min(len(c), 4)):
+            arr[k] = c[k]
+    return p
+
+
 class NBodyGPU:
     def __init__(self, device, particleData, stellarData=None):
         P = f32(particleData).ravel()
@@ -59,21 +78,9 @@ class NBodyGPU:
     def updateCentralMass(self, mass, idx=0):
         self._ok(lib().gs_update_central_mass(self._ctx, float(mass), int(idx)))
 
-    def updateParams(self, *, dt, G, epsilon, theta=0.5, haloMass=0, haloA=1, gasDrag=0, time=0,
-                     agingRate=25, sfDensity=1e9, sfEff=0, sfDt=0, haloCenters=()):
-        """NBodyGPU.js:253-275 (epsilon^2 in f32, N forced, at most two halo centres)."""
-        p = GsParams()
-        p.dt, p.G = dt, G
-        p.epsilon2 = float(np.float32(epsilon) * np.float32(epsilon))
-        p.N = self.N
-        p.theta, p.haloMass, p.haloA, p.gasDrag = theta, haloMass, haloA, gasDrag
-        p.time, p.agingRate, p.sfDensity, p.sfEff, p.sfDt = time, agingRate, sfDensity, sfEff, sfDt
-        hc = list(haloCenters or [])
-        p.haloCount = min(len(hc), 2)
-        for h, c in enumerate(hc[:2]):
-            arr = p.haloC1 if h == 0 else p.haloC2
-            for k in range(min(len(c), 4)):
-                arr[k] = c[k]
+    def updateParams(self, **kw):
+        """NBodyGPU.js:253-275 (keyword arguments of ``build_params``)."""
+        p = build_params(self.N, **kw)
         self._params = p
         self._ok(lib().gs_update_params(self._ctx, C.byref(p)))
 
@@ -164,6 +171,12 @@ class NBodyGPU:
 
     def run(self, nsteps: int, starFormation: bool = False):
         self._ok(lib().gs_run(self._ctx, int(nsteps), int(bool(starFormation))))
+
+    def stepKernels(self) -> int:
+        """Kernel launches per full step (nodes of the captured step graph)."""
+        n = C.c_uint32(0)
+        self._ok(lib().gs_step_kernels(self._ctx, C.byref(n)))
+        return n.value
 
     @property
     def stream(self) -> int:

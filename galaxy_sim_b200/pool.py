@@ -1,0 +1,176 @@
+"""Many independent galaxies in one context: batches and the serving pool.
+
+The reference runs one simulation per page (one NBodyGPU, one worker). Here a
+``GalaxyPool`` owns one ``gs_ctx`` pool: every resident galaxy is stepped by the
+same launches (segmented Morton sort, tree build, work-stealing walk) replayed
+from one CUDA graph per step, and each galaxy's result equals its solo run.
+Galaxies are admitted into free slots and free particle ranges and released
+when done, which is what continuous batching needs.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import GS_ENOMEM, GalaxyError, GsDiag, check, f32, lib, ptr
+from .nbody_gpu import build_params
+
+
+def device_memory(device: int = 0):
+    """(free, total) bytes of a CUDA device."""
+    f, t = C.c_uint64(0), C.c_uint64(0)
+    check(lib().gs_device_memory(int(device), C.byref(f), C.byref(t)))
+    return f.value, t.value
+
+
+def pool_bytes(capacity: int, max_galaxies: int) -> int:
+    """Device bytes of a pool for ``capacity`` particles and ``max_galaxies`` slots."""
+    return int(lib().gs_pool_bytes(int(capacity), int(max_galaxies)))
+
+
+def capacity_for_bytes(budget: int, max_galaxies: int) -> int:
+    """Largest particle capacity whose pool fits in ``budget`` bytes."""
+    lo, hi = 0, 1 << 27
+    while lo < hi:
+        mid = (lo + hi + 1) // 2
+        if pool_bytes(mid, max_galaxies) <= budget:
+            lo = mid
+        else:
+            hi = mid - 1
+    return lo
+
+
+class GalaxyPool:
+    def __init__(self, capacity: int, max_galaxies: int, device: int = 0):
+        h = C.c_void_p()
+        check(lib().gs_pool_create(int(device), int(capacity), int(max_galaxies), C.byref(h)))
+        self._ctx = h
+        self.capacity = int(capacity)
+        self.max_galaxies = int(max_galaxies)
+        self.device = int(device)
+        self.n = {}  # slot -> N
+
+    def _ok(self, rc):
+        check(rc, self._ctx)
+
+    def _sel(self, slot: int):
+        self._ok(lib().gs_select(self._ctx, int(slot)))
+
+    # -- admission -------------------------------------------------------------------------
+    def add(self, particles, stellar=None, params: dict | None = None, tracking=None):
+        """Admit a galaxy; returns its slot, or None when no slot / particle range is free.
+
+        ``params`` holds NBodyGPU.updateParams keywords; ``tracking`` is
+        (c1, c2, halo1, halo2) as in NBodyGPU.setTracking."""
+        P = f32(particles).reshape(-1, 8)
+        S = None if stellar is None else f32(stellar).reshape(-1, 4)
+        N = P.shape[0]
+        prm = build_params(N, **params) if params else None
+        slot = C.c_uint32(0)
+        rc = lib().gs_pool_add(self._ctx, N, ptr(P), ptr(S), None if prm is None else C.byref(prm),
+                               C.byref(slot))
+        if rc == GS_ENOMEM:
+            return None
+        self._ok(rc)
+        s = slot.value
+        self.n[s] = N
+        if tracking is not None:
+            self.set_tracking(s, *tracking)
+        return s
+
+    def remove(self, slot: int):
+        self._ok(lib().gs_pool_remove(self._ctx, int(slot)))
+        self.n.pop(int(slot), None)
+
+    def free(self):
+        """(largest free contiguous particle range, free slots)."""
+        r, s = C.c_uint64(0), C.c_uint32(0)
+        self._ok(lib().gs_pool_free(self._ctx, C.byref(r), C.byref(s)))
+        return r.value, s.value
+
+    def fits(self, N: int) -> bool:
+        r, s = self.free()
+        return s > 0 and r >= ((N + 255) // 256) * 256
+
+    # -- per-galaxy state ------------------------------------------------------------------
+    def set_params(self, slot: int, **kw):
+        self._sel(slot)
+        p = build_params(self.n[slot], **kw)
+        self._ok(lib().gs_update_params(self._ctx, C.byref(p)))
+
+    def set_tracking(self, slot: int, c1=-1, c2=-1, halo1=None, halo2=None):
+        self._sel(slot)
+        h1 = None if halo1 is None else np.asarray(halo1, np.float64)
+        h2 = None if halo2 is None else np.asarray(halo2, np.float64)
+        self._ok(lib().gs_set_tracking(self._ctx, int(c1), int(c2), ptr(h1), ptr(h2)))
+
+    def get_tracking(self, slot: int):
+        self._sel(slot)
+        c1, c2 = C.c_int64(), C.c_int64()
+        h1, h2 = np.zeros(3), np.zeros(3)
+        self._ok(lib().gs_get_tracking(self._ctx, C.byref(c1), C.byref(c2), ptr(h1), ptr(h2)))
+        return c1.value, c2.value, h1, h2
+
+    def read_state(self, slot: int):
+        self._sel(slot)
+        N = self.n[slot]
+        P = np.zeros((N, 8), np.float32)
+        S = np.zeros((N, 4), np.float32)
+        self._ok(lib().gs_read_state(self._ctx, ptr(P), ptr(S)))
+        return P, S
+
+    def write_state(self, slot: int, particles8=None, stellar4=None):
+        self._sel(slot)
+        P = None if particles8 is None else f32(particles8)
+        S = None if stellar4 is None else f32(stellar4)
+        self._ok(lib().gs_write_state(self._ctx, ptr(P), ptr(S)))
+
+    def energy(self, slot: int) -> dict:
+        self._sel(slot)
+        d = GsDiag()
+        self._ok(lib().gs_energy(self._ctx, C.byref(d)))
+        return {"e_diag": d.e_diag, "e_true": d.e_true, "momentum": list(d.momentum), "mass": d.mass}
+
+    def energies(self) -> np.ndarray:
+        """(max_galaxies, 6) array: e_diag, e_true, px, py, pz, mass of every slot."""
+        out = (GsDiag * self.max_galaxies)()
+        self._ok(lib().gs_pool_energies(self._ctx, out, self.max_galaxies))
+        return np.array([[d.e_diag, d.e_true, *d.momentum, d.mass] for d in out])
+
+    def device_errors(self, slot: int, clear=False) -> int:
+        self._sel(slot)
+        b = C.c_uint32(0)
+        self._ok(lib().gs_device_errors(self._ctx, C.byref(b), int(bool(clear))))
+        return b.value
+
+    # -- stepping --------------------------------------------------------------------------
+    def run(self, nsteps: int, star_formation: bool = False):
+        self._ok(lib().gs_run(self._ctx, int(nsteps), int(bool(star_formation))))
+
+    def sync(self, timeout_ns=0):
+        self._ok(lib().gs_sync(self._ctx, int(timeout_ns)))
+
+    @property
+    def stream(self) -> int:
+        d = C.c_void_p()
+        self._ok(lib().gs_stream(self._ctx, C.byref(d)))
+        return d.value or 0
+
+    @property
+    def particles(self) -> int:
+        return sum(self.n.values())
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            lib().gs_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+__all__ = ["GalaxyPool", "GalaxyError", "device_memory", "pool_bytes", "capacity_for_bytes"]

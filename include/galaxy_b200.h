@@ -108,7 +108,9 @@ int gs_set_com_mode(gs_ctx* ctx, int mode);
 /* NBodyGPU.updateCentralMass (NBodyGPU.js:245-251): both ping-pong buffers. */
 int gs_update_central_mass(gs_ctx* ctx, float mass, uint32_t idx);
 /* NBodyGPU.applyPermutation (NBodyGPU.js:225-238): gather out[i] = in[perm[i]] of
- * particles and stellar records, then flip both ping-pongs. perm is a host array. */
+ * particles and stellar records, then flip both ping-pongs. perm is a host array.
+ * In a pool holding other galaxies the gathered records are copied back into the
+ * current buffers instead of flipping them. */
 int gs_apply_permutation(gs_ctx* ctx, const uint32_t* perm);
 /* NBodyGPU.uploadBHTree (NBodyGPU.js:288-301): level_ranges holds n_levels
  * [start, count] pairs (at most 16, like the reference's refresh uniform). */
@@ -144,6 +146,9 @@ int gs_sort_build(gs_ctx* ctx);
  * formation when do_sf)], advancing Params.time by dt each step; replayed from a
  * CUDA graph. */
 int gs_run(gs_ctx* ctx, uint32_t nsteps, int do_sf);
+/* Kernel launches in one full step: the kernel nodes of the CUDA graph gs_run
+ * captured last (0 before the first gs_run). */
+int gs_step_kernels(gs_ctx* ctx, uint32_t* n);
 /* The context's CUDA stream (cudaStream_t), e.g. to record timing events in
  * its order. */
 int gs_stream(gs_ctx* ctx, void** stream);
@@ -186,6 +191,43 @@ int gs_sort_and_build(const float* particles8, const float* stellar4, uint32_t N
                       uint32_t* perm, gs_node* nodes, uint32_t max_nodes, uint32_t* num_nodes,
                       uint32_t* level_ranges, uint32_t lr_cap, uint32_t* n_levels,
                       int64_t* central_idx, int64_t* central_idx2, float* sorted_mass);
+
+/* ---- pools: many independent galaxies in one context ---------------------------------- */
+
+/* No counterpart in the reference, which runs one simulation per page. A context
+ * is a pool of galaxy slots over one set of device buffers; gs_sort_build,
+ * gs_step, gs_refresh, gs_star_formation and gs_run act on every resident galaxy
+ * at once, one launch per kernel (segmented sort, build and walk; a CUDA graph per
+ * step in gs_run). The per-galaxy entry points above (gs_update_params, gs_set_time,
+ * gs_update_central_mass, gs_apply_permutation, gs_upload_tree, gs_read_positions,
+ * gs_position_buffer, gs_stellar_buffer, gs_set_tracking, gs_get_tracking,
+ * gs_get_tree, gs_read_state, gs_write_state, gs_read_forces, gs_energy,
+ * gs_device_errors, gs_counters) act on the selected slot (gs_select, default 0)
+ * and use that galaxy's own indices. gs_create makes a pool holding one galaxy in
+ * slot 0. Each galaxy's results equal those of the same galaxy alone. */
+
+/* Free and total device memory of a CUDA device (cudaMemGetInfo). */
+int gs_device_memory(int device, uint64_t* free_bytes, uint64_t* total_bytes);
+/* Device bytes gs_pool_create allocates for a capacity (admission by free HBM;
+ * debug force buffers and BHNode staging come on demand on top). */
+uint64_t gs_pool_bytes(uint64_t particle_capacity, uint32_t max_galaxies);
+/* An empty pool for up to particle_capacity particles (in total, each galaxy
+ * rounded up to a multiple of 256) and max_galaxies galaxies. */
+int gs_pool_create(int device, uint64_t particle_capacity, uint32_t max_galaxies, gs_ctx** out);
+/* Admit a galaxy: N particles (N*8 floats), optional stellar records (NULL =
+ * zeros) and Params (NULL = zeros); its slot index is written to slot. Returns
+ * GS_ENOMEM when no slot or no contiguous particle range is free. */
+int gs_pool_add(gs_ctx* ctx, uint32_t N, const float* particles8, const float* stellar4,
+                const gs_params* params, uint32_t* slot);
+/* Release a galaxy's slot and particle range. */
+int gs_pool_remove(gs_ctx* ctx, uint32_t slot);
+/* Largest free contiguous particle range and number of free slots. */
+int gs_pool_free(gs_ctx* ctx, uint64_t* largest_range, uint32_t* free_slots);
+/* Select the slot the per-galaxy entry points act on. */
+int gs_select(gs_ctx* ctx, uint32_t slot);
+/* FP64 diagnostics of every slot's last walk (out[slot], zeros for empty slots),
+ * cap entries at most. */
+int gs_pool_energies(gs_ctx* ctx, gs_diag* out, uint32_t cap);
 
 /* ---- allocation-free sort ------------------------------------------------------------- */
 
