@@ -54,6 +54,10 @@ def parse():
     ap.add_argument("--theta", type=float, default=None)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--requests", type=int, default=32, help="serve: requests in the stream")
+    ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrival rate (1/s)")
+    ap.add_argument("--min-steps", type=int, default=100, help="serve: fewest steps of a request")
+    ap.add_argument("--max-steps", type=int, default=2000, help="serve: most steps of a request")
     return ap.parse_args()
 
 
@@ -368,11 +372,148 @@ def run_reference(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def batch96(seed=7):
+    """96 disks, N log-uniform in [4096, 262144], Q uniform in [1, 2], 2-4 arms,
+    gas fraction 0 or 0.3 (gas: drag + star formation), eps 0.02, theta 0.5,
+    dt 0.005."""
+    import math
+
+    import numpy as np
+
+    from galaxy_sim_b200 import initial_conditions as ic
+    from galaxy_sim_b200.simulation import Physics
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(96):
+        N = int(round(math.exp(rng.uniform(math.log(4096), math.log(262144)))))
+        Q = float(rng.uniform(1.0, 2.0))
+        arms = int(rng.integers(2, 5))
+        gas = float(rng.choice([0.0, 0.3]))
+        g = ic.galaxy_disk(N, 1000 + k, Q=Q, arms=arms, gas_frac=gas)
+        ph = Physics(0.02, 0.5, 0.005, gas_drag=0.25 if gas else 0.0, sf_eff=0.02 if gas else 0.0)
+        out.append((g, ph))
+    return out
+
+
+def _timed_steps(stream_ptr, local, K, step, flush):
+    """Device time (ms) of K calls of step(), each bracketed by CUDA events on
+    the given stream after an L2 flush, with a device-side gate in front."""
+    import torch
+
+    ext = torch.cuda.ExternalStream(stream_ptr, device=torch.device("cuda", local))
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    with torch.cuda.stream(ext):
+        torch.cuda._sleep(GATE_CYCLES)
+    for k in range(K):
+        with torch.cuda.stream(ext):
+            flush.fill_(float(k))
+            ev[k][0].record(ext)
+        step()
+        with torch.cuda.stream(ext):
+            ev[k][1].record(ext)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
+
+
+def run_batch(args, ws, rank, local):
+    """Batched ensemble (one pool, one graph per step) vs the same galaxies as
+    back-to-back plain runs, same GPU, same steps."""
+    import torch
+
+    from galaxy_sim_b200.nbody_gpu import NBodyGPU
+    from galaxy_sim_b200.pool import GalaxyPool
+    from galaxy_sim_b200.simulation import params_dict
+
+    torch.cuda.set_device(local)
+    gals = batch96()
+    Ntot = sum(g.N for g, _ in gals)
+    K, W = args.steps, args.warmup
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+    pool = GalaxyPool(sum((g.N + 255) // 256 * 256 for g, _ in gals), len(gals), local)
+    for g, ph in gals:
+        pool.add(g.particles, g.stellar, params_dict(g, ph), star_formation=ph.sf_eff > 0)
+    pool.run(W, True)
+    pool.sync()
+    with Clocks(local) as clk:
+        bms = _timed_steps(pool.stream, local, K, lambda: pool.run(1, True), flush)
+    clocks = clk.summary()
+    E = pool.energies()
+    pool.close()
+    # the same galaxies, one after another, each in its own single-galaxy context
+    pms = 0.0
+    plain_steps = []
+    for g, ph in gals:
+        sim = NBodyGPU(local, g.particles, g.stellar)
+        sim.updateParams(**params_dict(g, ph))
+        sf = ph.sf_eff > 0
+        sim.run(W, sf)
+        sim.sync()
+        t = _timed_steps(sim.stream, local, K, lambda: sim.run(1, sf), flush)
+        pms += sum(t)
+        plain_steps.append(sum(t) / K)
+        sim.destroy()
+    b_total = sum(bms)
+    srt = sorted(bms)
+    value = Ntot * K / (b_total / 1e3)
+    plain = Ntot * K / (pms / 1e3)
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W,
+        "ms_per_step": round(b_total / K, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ICs)",
+        "config": {"workload": "batch96", "galaxies": len(gals), "N_total": Ntot,
+                   "N_range": [min(g.N for g, _ in gals), max(g.N for g, _ in gals)],
+                   "theta": 0.5, "epsilon": 0.02, "dt": 0.005, "bucket": 16,
+                   "l2": "flush 256 MiB between timed steps"},
+        "latency_ms": {"p50": srt[len(srt) // 2], "p99": srt[min(len(srt) - 1, int(0.99 * len(srt)))]},
+        "plain_back_to_back": {"value": round(plain, 1), "ms_per_step_all_galaxies": round(pms / K, 4),
+                               "ms_per_step_p50_galaxy": round(sorted(plain_steps)[len(plain_steps) // 2], 4)},
+        "batched_over_plain": round(value / plain, 3),
+        "finite_diagnostics": bool(torch.isfinite(torch.tensor(E)).all()),
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args, ws, rank, local):
+    """Served stream (Poisson arrivals) through the continuous-batching server
+    and through the one-at-a-time server on the same GPU."""
+    import torch
+
+    from galaxy_sim_b200.serve import BatchServer, PlainServer, make_stream
+
+    torch.cuda.set_device(local)
+    n_req = args.requests
+    reqs = make_stream(n_req, args.rate, seed=11, step_range=(args.min_steps, args.max_steps))
+    srv = BatchServer(max_galaxies=64, device=local)
+    with Clocks(local) as clk:
+        b = srv.serve(reqs)
+    clocks = clk.summary()
+    srv.close()
+    reqs2 = make_stream(n_req, args.rate, seed=11, step_range=(args.min_steps, args.max_steps))
+    p = PlainServer(local).serve(reqs2)
+    line = {
+        "metric": METRIC, "value": b["value"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ICs)",
+        "config": {"workload": "serve", "requests": n_req, "rate_per_s": args.rate,
+                   "N_range": [8192, 1 << 20], "steps_range": [args.min_steps, args.max_steps],
+                   "presets": ["disk", "sphere", "collision"], "eps": [0.02, 0.05], "theta": [0.5, 0.7],
+                   "dt": [0.0025, 0.005]},
+        "batched": b, "plain": p, "batched_over_plain": round(b["value"] / p["value"], 3),
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
     if args.impl == "reference":
         run_reference(args, ws, rank, local)
+    elif args.workload == "batch96":
+        run_batch(args, ws, rank, local)
+    elif args.workload == "serve":
+        run_serve(args, ws, rank, local)
     else:
         run_ours(args, ws, rank, local)
 

@@ -30,7 +30,7 @@ struct __align__(16) DevState {
   double halo_c[2][3];    // smoothed halo centres (main.js haloCenters, doubles)
   long long central[2];   // tracked central particles (particle-pool indices), -1 = none
   unsigned int err;       // GS_DERR_* bits
-  unsigned int pad_;
+  unsigned int sf_off;    // nonzero: this galaxy skips star formation
   unsigned long long counters[3];  // monopoles, leaf pairs, node visits
 };
 

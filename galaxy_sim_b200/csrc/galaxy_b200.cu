@@ -506,6 +506,8 @@ void enqueue_walk(gs_ctx* c, int sf) {
   a.partials = c->partials;
   a.work = c->walk_work;
   a.L = c->lay;
+  a.pool_n = (uint32_t)c->plan.cap;
+  a.node_pool = (uint32_t)c->plan.nodes;
   const uint32_t g = c->walk_grid;
   cudaStream_t s = c->stream;
   const bool one = c->lay.nseg == 1;
@@ -912,6 +914,16 @@ int gs_set_time(gs_ctx* ctx, double t) {
   (void)s;
   CK(ctx, cudaStreamSynchronize(ctx->stream), "sync");
   CK(ctx, cudaMemcpy(&ctx->st[ctx->sel].sim_time, &t, sizeof(double), cudaMemcpyHostToDevice), "time");
+  return GS_OK;
+}
+
+int gs_set_star_formation(gs_ctx* ctx, int enable) {
+  CTX_CHECK(ctx);
+  SLOT(ctx, s);
+  (void)s;
+  CK(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+  const unsigned off = enable ? 0u : 1u;
+  CK(ctx, cudaMemcpy(&ctx->st[ctx->sel].sf_off, &off, sizeof(off), cudaMemcpyHostToDevice), "sf flag");
   return GS_OK;
 }
 

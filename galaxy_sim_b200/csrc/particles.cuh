@@ -252,6 +252,7 @@ __global__ void __launch_bounds__(kTileThreads)
     sf_kernel(float4* __restrict__ P, float4* __restrict__ S, Layout L,
               const DevState* __restrict__ st) {
   const TileRange t = tile_range(L, blockIdx.x);
+  if (st[t.slot].sf_off) return;
   const gs_params prm = st[t.slot].p;
 #pragma unroll
   for (int q = 0; q < kTilePer; q++) {

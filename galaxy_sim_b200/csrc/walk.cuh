@@ -105,6 +105,7 @@ struct WalkArgs {
   double* __restrict__ partials;    // [groups][kPartials]
   unsigned* work;                   // [0] next group, [1] finished warps (self-resetting)
   Layout L;                         // galaxies and the group -> galaxy map
+  uint32_t pool_n, node_pool;       // particle and node pool sizes (memory-safety bounds)
   SegDesc seg0;                     // the only galaxy, for the one-galaxy instantiation
 };
 
@@ -205,7 +206,6 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
     const float qe2 = 0.25f * eps2;
     const bool soft = eps2 > 0.0f;  // self pairs may then be summed and removed afterwards
     const uint32_t seg_end = sd.off + sd.n;
-    const uint32_t node_end = sd.node_off + sd.node_cap;
     const uint32_t gbeg = sd.off + (gcur - sd.group0) * kWalkGroup, gend = gbeg + kWalkGroup;
     const uint32_t i = gbeg + lane;
     const bool valid = i < seg_end;
@@ -323,7 +323,9 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
         const unsigned open = __ballot_sync(full, (obits >> cc) & 1u);
         const uint4 mt = S.cmeta[cc];
         const uint32_t cchild = mt.x, ccnt = mt.y & ~kLeafBit;
-        if (!(cchild > start + cc && (uint64_t)cchild + ccnt <= node_end && ccnt >= 1u && ccnt <= 8u)) {
+        // a galaxy's child ranges stay in its node range by construction (build,
+        // upload check); the walk itself only guards the pool bounds
+        if (!(cchild > start + cc && (uint64_t)cchild + ccnt <= a.node_pool && ccnt >= 1u && ccnt <= 8u)) {
           if (lane == 0) raise_err(sst, GS_DERR_TREE);
           continue;
         }
@@ -345,7 +347,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
         const uint32_t cc = __ffs(bb) - 1;
         const uint4 mt = S.cmeta[cc];
         const uint32_t ccnt = mt.y & ~kLeafBit;
-        if (mt.x < sd.off || (uint64_t)mt.x + ccnt > seg_end) {
+        if ((uint64_t)mt.x + ccnt > a.pool_n) {
           if (lane == 0) raise_err(sst, GS_DERR_TREE);
           continue;
         }
@@ -456,7 +458,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
       my = m * vy;
       mz = m * vz;
       ms = m;
-      if (SF) {
+      if (SF && !sst->sf_off) {
         float4 s = a.stellar[i];
         const float4 s_old = s;
         star_formation_one(P, i - sd.off, o1, s);

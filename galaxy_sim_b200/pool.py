@@ -58,11 +58,13 @@ class GalaxyPool:
         self._ok(lib().gs_select(self._ctx, int(slot)))
 
     # -- admission -------------------------------------------------------------------------
-    def add(self, particles, stellar=None, params: dict | None = None, tracking=None):
+    def add(self, particles, stellar=None, params: dict | None = None, tracking=None,
+            star_formation: bool = True):
         """Admit a galaxy; returns its slot, or None when no slot / particle range is free.
 
         ``params`` holds NBodyGPU.updateParams keywords; ``tracking`` is
-        (c1, c2, halo1, halo2) as in NBodyGPU.setTracking."""
+        (c1, c2, halo1, halo2) as in NBodyGPU.setTracking; ``star_formation``
+        False keeps run(..., star_formation=True) from acting on this galaxy."""
         P = f32(particles).reshape(-1, 8)
         S = None if stellar is None else f32(stellar).reshape(-1, 4)
         N = P.shape[0]
@@ -77,6 +79,9 @@ class GalaxyPool:
         self.n[s] = N
         if tracking is not None:
             self.set_tracking(s, *tracking)
+        if not star_formation:
+            self._sel(s)
+            self._ok(lib().gs_set_star_formation(self._ctx, 0))
         return s
 
     def remove(self, slot: int):

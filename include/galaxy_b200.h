@@ -105,6 +105,10 @@ int gs_set_time(gs_ctx* ctx, double t);
 /* COM arithmetic of the on-device build's refresh: 0 = FP32 like refresh_level
  * (nbody_bh.wgsl:289-313), 2 = FP32 leaves with FP64 internal-node sums. */
 int gs_set_com_mode(gs_ctx* ctx, int mode);
+/* Whether star formation (gs_star_formation, and gs_run with do_sf) acts on
+ * this galaxy; on by default, as the reference encodes it every frame. Off lets
+ * galaxies with and without star formation share a pool. */
+int gs_set_star_formation(gs_ctx* ctx, int enable);
 /* NBodyGPU.updateCentralMass (NBodyGPU.js:245-251): both ping-pong buffers. */
 int gs_update_central_mass(gs_ctx* ctx, float mass, uint32_t idx);
 /* NBodyGPU.applyPermutation (NBodyGPU.js:225-238): gather out[i] = in[perm[i]] of

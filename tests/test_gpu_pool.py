@@ -108,6 +108,19 @@ def test_admission_into_holes_keeps_results(gpu_lib):
     pool.close()
 
 
+def test_star_formation_switch_per_galaxy(gpu_lib):
+    """A galaxy admitted with star formation off stays exactly its run without
+    star formation while a neighbour forms stars in the same steps."""
+    (g0, p0), _, _, (g3, p3), _ = _cases()
+    pool = GalaxyPool(g0.N + g3.N + 512, 2)
+    a = pool.add(g0.particles, g0.stellar, params_dict(g0, p0))
+    b = pool.add(g3.particles, g3.stellar, params_dict(g3, p3), _tracking(g3), star_formation=False)
+    pool.run(3, True)
+    _check_same(pool, a, _solo(g0, p0, 3, True))
+    _check_same(pool, b, _solo(g3, p3, 3, False))
+    pool.close()
+
+
 def test_pool_accounting(gpu_lib):
     assert pool_bytes(1 << 20, 16) > pool_bytes(1 << 19, 16) > 0
     pool = GalaxyPool(10000, 2)
