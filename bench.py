@@ -19,6 +19,15 @@ metric through the C ABI with pinned host buffers: upload of the initial
 state, per step a Params upload and an energy-diagnostic readback, and a final
 state readback, all inside the event-timed region.
 
+The same line carries the metric's batched and served halves (one GPU):
+``batched`` = 96 disks (N log-uniform in [4096, 262144]) stepped as one pool,
+one CUDA graph per step, against the same galaxies run back to back in plain
+single-galaxy contexts; ``served`` = a seeded Poisson stream of simulation
+requests (disk / sphere / collision presets, N log-uniform in [8192, 2^20])
+through the continuous-batching server and through a one-at-a-time server,
+with per-step and per-request p50/p99 latency and admission queue wait.
+``--workload batch96`` and ``--workload serve`` print those alone.
+
 ``--impl reference`` times the reference algorithm on the host cores: the CPU
 restatement in oracle/ (sort + build single-threaded like the reference's Web
 Worker, refresh + walk + kick-drift on all cores), each step a bounded sample.
@@ -37,7 +46,8 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "particle-steps/s (full sort+build+refresh+walk+integrate step)"
+METRIC = "particle-steps/s at N=500k \u03b8=0.5; batched/served vs plain, p50/p99, same GPU"
+WALK_PROFILE = os.path.join(ROOT, "profiles", "walk_kernel_disk512k.md")
 UNIT = "particle-steps/s"
 FLOPS_PER_INTERACTION = 23
 L2_FLUSH_BYTES = 256 << 20
@@ -54,7 +64,8 @@ def parse():
     ap.add_argument("--theta", type=float, default=None)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--requests", type=int, default=32, help="serve: requests in the stream")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched/served comparison")
+    ap.add_argument("--requests", type=int, default=16, help="serve: requests in the stream")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrival rate (1/s)")
     ap.add_argument("--min-steps", type=int, default=100, help="serve: fewest steps of a request")
     ap.add_argument("--max-steps", type=int, default=2000, help="serve: most steps of a request")
@@ -243,7 +254,9 @@ def run_ours(args, ws, rank, local):
                 "algorithmic": f"{interactions / N:.1f} interactions/particle x {N} particles x "
                                f"{FLOPS_PER_INTERACTION} flops per launch",
                 "walk_ms": round(walk_avg, 4), "sort_build_refresh_ms": round(sum(build_ms) / R, 4),
-                "traffic": None}
+                "traffic": walk_traffic(w.name, w.physics.theta),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch "
+                                  "(profiles/walk_kernel_disk512k.md)"}
 
     # ---- e2e through the C ABI with pinned host buffers ----
     e2e = None
@@ -295,6 +308,12 @@ def run_ours(args, ws, rank, local):
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(w, g, steps=5, warmup=1, budget_s=15.0)
     sim.close()
+    batched = served = None
+    if ws == 1 and not args.no_batch:
+        # the metric's batched/served halves: 96 galaxies in one pool vs back-to-back
+        # plain runs, and a Poisson request stream through both servers
+        batched = batch_compare(local, min(K, 100), max(3, min(args.warmup, 5)))
+        served = serve_compare(local, args.requests, args.rate, args.min_steps, args.max_steps)
     if dist:
         dist.destroy_process_group()
     if rank != 0:
@@ -311,6 +330,7 @@ def run_ours(args, ws, rank, local):
         "interactions_per_particle": round(interactions / N, 2),
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": K * n_launch_step,
+        "batched": batched, "served": served,
     }
     print(json.dumps(line), flush=True)
 
@@ -416,7 +436,21 @@ def _timed_steps(stream_ptr, local, K, step, flush):
     return [a.elapsed_time(b) for a, b in ev]
 
 
-def run_batch(args, ws, rank, local):
+def walk_traffic(workload: str, theta: float):
+    """DRAM bytes per walk launch from the committed ncu summary (disk512k, theta 0.5)."""
+    import re
+
+    if workload != "disk512k" or theta != 0.5:
+        return None
+    try:
+        m = re.search(r"dram__bytes_read.sum \+ dram__bytes_write.sum \| ([0-9.]+) MB \+ ([0-9.]+) MB",
+                      open(WALK_PROFILE).read())
+    except OSError:
+        return None
+    return int(round((float(m.group(1)) + float(m.group(2))) * 1e6)) if m else None
+
+
+def batch_compare(local, K, W):
     """Batched ensemble (one pool, one graph per step) vs the same galaxies as
     back-to-back plain runs, same GPU, same steps."""
     import torch
@@ -428,7 +462,6 @@ def run_batch(args, ws, rank, local):
     torch.cuda.set_device(local)
     gals = batch96()
     Ntot = sum(g.N for g, _ in gals)
-    K, W = args.steps, args.warmup
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
     pool = GalaxyPool(sum((g.N + 255) // 256 * 256 for g, _ in gals), len(gals), local)
     for g, ph in gals:
@@ -457,25 +490,24 @@ def run_batch(args, ws, rank, local):
     srt = sorted(bms)
     value = Ntot * K / (b_total / 1e3)
     plain = Ntot * K / (pms / 1e3)
-    line = {
-        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W,
-        "ms_per_step": round(b_total / K, 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ICs)",
+    return {
+        "value": round(value, 1), "unit": UNIT, "steps": K, "warmup": W,
+        "ms_per_step": round(b_total / K, 4),
         "config": {"workload": "batch96", "galaxies": len(gals), "N_total": Ntot,
                    "N_range": [min(g.N for g, _ in gals), max(g.N for g, _ in gals)],
                    "theta": 0.5, "epsilon": 0.02, "dt": 0.005, "bucket": 16,
                    "l2": "flush 256 MiB between timed steps"},
-        "latency_ms": {"p50": srt[len(srt) // 2], "p99": srt[min(len(srt) - 1, int(0.99 * len(srt)))]},
+        "latency_ms": {"p50": round(srt[len(srt) // 2], 4),
+                       "p99": round(srt[min(len(srt) - 1, int(0.99 * len(srt)))], 4)},
         "plain_back_to_back": {"value": round(plain, 1), "ms_per_step_all_galaxies": round(pms / K, 4),
                                "ms_per_step_p50_galaxy": round(sorted(plain_steps)[len(plain_steps) // 2], 4)},
         "batched_over_plain": round(value / plain, 3),
         "finite_diagnostics": bool(torch.isfinite(torch.tensor(E)).all()),
         "clocks": clocks,
     }
-    print(json.dumps(line), flush=True)
 
 
-def run_serve(args, ws, rank, local):
+def serve_compare(local, n_req, rate, min_steps, max_steps):
     """Served stream (Poisson arrivals) through the continuous-batching server
     and through the one-at-a-time server on the same GPU."""
     import torch
@@ -483,26 +515,41 @@ def run_serve(args, ws, rank, local):
     from galaxy_sim_b200.serve import BatchServer, PlainServer, make_stream
 
     torch.cuda.set_device(local)
-    n_req = args.requests
-    reqs = make_stream(n_req, args.rate, seed=11, step_range=(args.min_steps, args.max_steps))
+    reqs = make_stream(n_req, rate, seed=11, step_range=(min_steps, max_steps))
     srv = BatchServer(max_galaxies=64, device=local)
     with Clocks(local) as clk:
         b = srv.serve(reqs)
     clocks = clk.summary()
     srv.close()
-    reqs2 = make_stream(n_req, args.rate, seed=11, step_range=(args.min_steps, args.max_steps))
+    reqs2 = make_stream(n_req, rate, seed=11, step_range=(min_steps, max_steps))
     p = PlainServer(local).serve(reqs2)
-    line = {
-        "metric": METRIC, "value": b["value"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ICs)",
-        "config": {"workload": "serve", "requests": n_req, "rate_per_s": args.rate,
-                   "N_range": [8192, 1 << 20], "steps_range": [args.min_steps, args.max_steps],
-                   "presets": ["disk", "sphere", "collision"], "eps": [0.02, 0.05], "theta": [0.5, 0.7],
-                   "dt": [0.0025, 0.005]},
-        "batched": b, "plain": p, "batched_over_plain": round(b["value"] / p["value"], 3),
-        "clocks": clocks,
-    }
-    print(json.dumps(line), flush=True)
+    return {"value": b["value"], "unit": UNIT,
+            "config": {"workload": "serve", "requests": n_req, "rate_per_s": rate,
+                       "N_range": [8192, 1 << 20], "steps_range": [min_steps, max_steps],
+                       "presets": ["disk", "sphere", "collision"], "eps": [0.02, 0.05],
+                       "theta": [0.5, 0.7], "dt": [0.0025, 0.005]},
+            "batched": b, "plain": p, "batched_over_plain": round(b["value"] / p["value"], 3),
+            "clocks": clocks}
+
+
+def _mode_line(d):
+    line = {"metric": METRIC, "value": d["value"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ICs)"}
+    line.update({k: v for k, v in d.items() if k not in ("value", "unit")})
+    return line
+
+
+def run_batch(args, ws, rank, local):
+    if rank != 0:
+        return
+    print(json.dumps(_mode_line(batch_compare(local, args.steps, args.warmup))), flush=True)
+
+
+def run_serve(args, ws, rank, local):
+    if rank != 0:
+        return
+    d = serve_compare(local, args.requests, args.rate, args.min_steps, args.max_steps)
+    print(json.dumps(_mode_line(d)), flush=True)
 
 
 def main():
