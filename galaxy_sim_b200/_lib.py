@@ -62,6 +62,7 @@ SIGNATURES = [
     ("gs_set_time", _int, [_vp, _f64]),
     ("gs_set_com_mode", _int, [_vp, _int]),
     ("gs_set_star_formation", _int, [_vp, _int]),
+    ("gs_set_walk_mode", _int, [_vp, _int]),
     ("gs_update_central_mass", _int, [_vp, _f32, _u32]),
     ("gs_apply_permutation", _int, [_vp, _vp]),
     ("gs_upload_tree", _int, [_vp, _vp, _u32, _vp, _u32]),

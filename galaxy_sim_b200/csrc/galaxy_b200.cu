@@ -215,6 +215,7 @@ struct gs_ctx {
   uint32_t sel = 0;
   bool single = false;  // created by gs_create: one galaxy, node pool 2N + 4096
   int com_mode = kComF32;
+  bool walk_comp = false;  // Kahan-compensated far-field sums in the walk
   void* host_stage = nullptr;  // pinned: [slots] params
   std::map<int, cudaGraphExec_t> graphs;
   uint32_t step_kernels = 0;  // kernel nodes of the last captured step graph
@@ -513,16 +514,27 @@ void enqueue_walk(gs_ctx* c, int sf) {
   const bool one = c->lay.nseg == 1;
   if (one) a.seg0 = c->seg_host[0];
   else memset(&a.seg0, 0, sizeof(a.seg0));
-  const int v = (sf ? 1 : 0) | (c->debug ? 2 : 0) | (one ? 4 : 0);
+  const int v = (sf ? 1 : 0) | (c->debug ? 2 : 0) | (one ? 4 : 0) | (c->walk_comp ? 8 : 0);
   switch (v) {
-    case 0: walk_kernel<false, false, false><<<g, kWalkThreads, 0, s>>>(a); break;
-    case 1: walk_kernel<true, false, false><<<g, kWalkThreads, 0, s>>>(a); break;
-    case 2: walk_kernel<false, true, false><<<g, kWalkThreads, 0, s>>>(a); break;
-    case 3: walk_kernel<true, true, false><<<g, kWalkThreads, 0, s>>>(a); break;
-    case 4: walk_kernel<false, false, true><<<g, kWalkThreads, 0, s>>>(a); break;
-    case 5: walk_kernel<true, false, true><<<g, kWalkThreads, 0, s>>>(a); break;
-    case 6: walk_kernel<false, true, true><<<g, kWalkThreads, 0, s>>>(a); break;
-    default: walk_kernel<true, true, true><<<g, kWalkThreads, 0, s>>>(a); break;
+#define GS_WALK_CASE(V, SF, DBG, ONE, COMP) \
+  case V: walk_kernel<SF, DBG, ONE, COMP><<<g, kWalkThreads, 0, s>>>(a); break;
+    GS_WALK_CASE(0, false, false, false, false)
+    GS_WALK_CASE(1, true, false, false, false)
+    GS_WALK_CASE(2, false, true, false, false)
+    GS_WALK_CASE(3, true, true, false, false)
+    GS_WALK_CASE(4, false, false, true, false)
+    GS_WALK_CASE(5, true, false, true, false)
+    GS_WALK_CASE(6, false, true, true, false)
+    GS_WALK_CASE(7, true, true, true, false)
+    GS_WALK_CASE(8, false, false, false, true)
+    GS_WALK_CASE(9, true, false, false, true)
+    GS_WALK_CASE(10, false, true, false, true)
+    GS_WALK_CASE(11, true, true, false, true)
+    GS_WALK_CASE(12, false, false, true, true)
+    GS_WALK_CASE(13, true, false, true, true)
+    GS_WALK_CASE(14, false, true, true, true)
+    GS_WALK_CASE(15, true, true, true, true)
+#undef GS_WALK_CASE
   }
   // per-galaxy FP64 diagnostics of this walk
   diag_reduce_kernel<<<c->lay.diag_chunks, dim3(32, kPartials), 0, s>>>(c->partials, c->lay, c->diag_chunk,
@@ -1131,13 +1143,22 @@ int gs_set_com_mode(gs_ctx* ctx, int mode) {
   return GS_OK;
 }
 
+int gs_set_walk_mode(gs_ctx* ctx, int compensated) {
+  CTX_CHECK(ctx);
+  if (compensated != 0 && compensated != 1) return ctx->fail(GS_EINVAL, "walk mode %d", compensated);
+  ctx->walk_comp = compensated != 0;
+  ctx->drop_graphs();
+  return GS_OK;
+}
+
 int gs_run(gs_ctx* ctx, uint32_t nsteps, int do_sf) {
   CTX_CHECK(ctx);
   int rc = ensure_layout(ctx);
   if (rc) return rc;
   if (!ctx->lay.nseg) return GS_OK;
   for (uint32_t s = 0; s < nsteps; s++) {
-    const int key = (ctx->cur) | (ctx->scur << 1) | ((do_sf ? 1 : 0) << 2) | ((ctx->debug ? 1 : 0) << 3);
+    const int key = (ctx->cur) | (ctx->scur << 1) | ((do_sf ? 1 : 0) << 2) | ((ctx->debug ? 1 : 0) << 3) |
+                    ((ctx->walk_comp ? 1 : 0) << 4);
     auto it = ctx->graphs.find(key);
     if (it == ctx->graphs.end()) {
       const int cur0 = ctx->cur, scur0 = ctx->scur;

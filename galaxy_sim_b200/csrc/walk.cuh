@@ -171,6 +171,15 @@ __device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k
 
 __device__ inline float2 f2(float a) { return make_float2(a, a); }
 
+// Kahan step on packed pairs: s + x with the lost low-order part kept in c
+// (c holds the negated error; the compensated total is s - c).
+__device__ __forceinline__ void kahan_add2(float2& s, float2& c, float2 x) {
+  const float2 y = __ffma2_rn(c, f2(-1.0f), x);   // x - c
+  const float2 t = __fadd2_rn(s, y);
+  c = __ffma2_rn(y, f2(-1.0f), __ffma2_rn(s, f2(-1.0f), t));  // (t - s) - y
+  s = t;
+}
+
 // 1.0f if a > b else 0.0f (ordered compare: NaN gives 0), as one compare-and-set.
 __device__ inline float set_gt(float a, float b) {
   float r;
@@ -183,8 +192,10 @@ __device__ inline void prefetch_l1(const void* p) {
 }
 
 // ONE: the layout holds a single galaxy, whose descriptor comes with the
-// kernel parameters instead of a per-group lookup.
-template <bool SF, bool DBG, bool ONE>
+// kernel parameters instead of a per-group lookup. COMP: far-field (monopole)
+// contributions are summed with Kahan compensation; near-field leaf sums add
+// plainly into the same sums.
+template <bool SF, bool DBG, bool ONE, bool COMP>
 __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(WalkArgs a) {
   __shared__ WalkSmem smem_all[kWalkWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -216,6 +227,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
     }
     const float2 px = f2(-p0.x), py = f2(-p0.y), pz = f2(-p0.z);  // negated: r = q + (-p)
     float2 ax = f2(0.f), ay = f2(0.f), az = f2(0.f), pt = f2(0.f);
+    float2 cax = f2(0.f), cay = f2(0.f), caz = f2(0.f), cpt = f2(0.f);  // COMP only
     float dens = 0.f, selfw = 0.f;
     unsigned long long nmono = 0, npair = 0, nvisit = 0;
     const unsigned all = __ballot_sync(full, valid);
@@ -293,10 +305,17 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
         const float2 rinv = __fmul2_rn(make_float2(rsqrtf(d2.x), rsqrtf(d2.y)), w);
         const float2 mr = __fmul2_rn(qm, rinv);
         const float2 f = __fmul2_rn(__fmul2_rn(mr, rinv), rinv);
-        ax = __ffma2_rn(rx, f, ax);
-        ay = __ffma2_rn(ry, f, ay);
-        az = __ffma2_rn(rz, f, az);
-        pt = __fadd2_rn(pt, mr);  // sum of m/r; potential = -G * sum
+        if (COMP) {
+          kahan_add2(ax, cax, __fmul2_rn(rx, f));
+          kahan_add2(ay, cay, __fmul2_rn(ry, f));
+          kahan_add2(az, caz, __fmul2_rn(rz, f));
+          kahan_add2(pt, cpt, mr);
+        } else {
+          ax = __ffma2_rn(rx, f, ax);
+          ay = __ffma2_rn(ry, f, ay);
+          az = __ffma2_rn(rz, f, az);
+          pt = __fadd2_rn(pt, mr);  // sum of m/r; potential = -G * sum
+        }
       }
       // bitmask of the children this lane opens (active, accept weight 0)
       uint32_t obits = 0;
@@ -406,6 +425,12 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
                    az, pt, selfw, npair, DBG);
         }
       }
+    }
+    if (COMP) {  // fold the compensations into the sums
+      ax = __ffma2_rn(cax, f2(-1.0f), ax);
+      ay = __ffma2_rn(cay, f2(-1.0f), ay);
+      az = __ffma2_rn(caz, f2(-1.0f), az);
+      pt = __ffma2_rn(cpt, f2(-1.0f), pt);
     }
     if (soft && selfw != 0.0f) pt.x -= selfw * p0.w * rsqrtf(eps2);
 

@@ -163,6 +163,10 @@ class NBodyGPU:
     def setTime(self, t: float):
         self._ok(lib().gs_set_time(self._ctx, float(t)))
 
+    def setWalkMode(self, compensated: bool):
+        """Kahan-compensated far-field sums in the walk (precision study)."""
+        self._ok(lib().gs_set_walk_mode(self._ctx, int(bool(compensated))))
+
     def setComMode(self, mode: int):
         self._ok(lib().gs_set_com_mode(self._ctx, int(mode)))
 

@@ -109,6 +109,10 @@ int gs_set_com_mode(gs_ctx* ctx, int mode);
  * this galaxy; on by default, as the reference encodes it every frame. Off lets
  * galaxies with and without star formation share a pool. */
 int gs_set_star_formation(gs_ctx* ctx, int enable);
+/* Walk arithmetic: 0 = plain FP32 sums (default), 1 = far-field (monopole)
+ * contributions summed with Kahan compensation. Together with gs_set_com_mode
+ * this selects the precision variant; no counterpart in the reference. */
+int gs_set_walk_mode(gs_ctx* ctx, int compensated);
 /* NBodyGPU.updateCentralMass (NBodyGPU.js:245-251): both ping-pong buffers. */
 int gs_update_central_mass(gs_ctx* ctx, float mass, uint32_t idx);
 /* NBodyGPU.applyPermutation (NBodyGPU.js:225-238): gather out[i] = in[perm[i]] of
