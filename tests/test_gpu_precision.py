@@ -10,8 +10,9 @@ Each is measured three ways: |da|/|a| against the FP64 walk of the same
 acceptance rule on the same tree, against a direct FP64 O(N^2) sum over a seeded
 32768-particle subset, and the drift of the true energy over STEPS steps
 (tracked halos, tree rebuilt every step). The halos move with the black holes,
-so this system's energy changes physically; the variants must agree on it. GPU FP64 is used only by the
-internal-node COM sums (com64) and the energy/momentum diagnostics.
+so this system's energy changes physically; the variants must agree on it.
+GPU FP64 is used only by the internal-node COM sums (com64) and the
+energy/momentum diagnostics.
 The figures are printed and, when a gpurun_out/ folder exists, written to
 gpurun_out/precision.json.
 """
