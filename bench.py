@@ -455,6 +455,7 @@ def batch_compare(local, K, W):
     back-to-back plain runs, same GPU, same steps."""
     import torch
 
+    from galaxy_sim_b200.autotune import autotune
     from galaxy_sim_b200.nbody_gpu import NBodyGPU
     from galaxy_sim_b200.pool import GalaxyPool
     from galaxy_sim_b200.simulation import params_dict
@@ -468,6 +469,8 @@ def batch_compare(local, K, W):
         pool.add(g.particles, g.stellar, params_dict(g, ph), star_formation=ph.sf_eff > 0)
     pool.run(W, True)
     pool.sync()
+    # launch knobs (walk grid, sort tile) picked by timing this batch; results do not depend on them
+    tuned = autotune(pool, steps=5, warmup=2, star_formation=True, device=local)
     with Clocks(local) as clk:
         bms = _timed_steps(pool.stream, local, K, lambda: pool.run(1, True), flush)
     clocks = clk.summary()
@@ -502,6 +505,7 @@ def batch_compare(local, K, W):
         "plain_back_to_back": {"value": round(plain, 1), "ms_per_step_all_galaxies": round(pms / K, 4),
                                "ms_per_step_p50_galaxy": round(sorted(plain_steps)[len(plain_steps) // 2], 4)},
         "batched_over_plain": round(value / plain, 3),
+        "autotune": tuned,
         "finite_diagnostics": bool(torch.isfinite(torch.tensor(E)).all()),
         "clocks": clocks,
     }

@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "libgalaxy_b200.so")
 
 GS_OK, GS_EINVAL, GS_ENOMEM, GS_ECUDA, GS_ETIMEDOUT, GS_EDEVICE, GS_ENOTREADY = 0, -1, -2, -3, -4, -5, -6
 DERR_LOOKBACK, DERR_STACK, DERR_NODES, DERR_TREE = 0x1, 0x2, 0x4, 0x8
+TUNE_WALK_BLOCKS_PER_SM, TUNE_SORT_ITEMS = 1, 2
 
 NODE_DTYPE = np.dtype([
     ("com", "<f4", (3,)), ("mass", "<f4"), ("size", "<f4"), ("isLeaf", "<u4"),
@@ -63,6 +64,8 @@ SIGNATURES = [
     ("gs_set_com_mode", _int, [_vp, _int]),
     ("gs_set_star_formation", _int, [_vp, _int]),
     ("gs_set_walk_mode", _int, [_vp, _int]),
+    ("gs_set_tuning", _int, [_vp, _int, _int]),
+    ("gs_get_tuning", _int, [_vp, _int, _vp]),
     ("gs_update_central_mass", _int, [_vp, _f32, _u32]),
     ("gs_apply_permutation", _int, [_vp, _vp]),
     ("gs_upload_tree", _int, [_vp, _vp, _u32, _vp, _u32]),

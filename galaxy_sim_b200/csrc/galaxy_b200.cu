@@ -68,7 +68,7 @@ Plan make_plan(uint64_t cap, uint32_t slots) {
   p.cap = cap;
   p.slots = slots;
   p.nodes = 2 * cap + 4096;
-  p.sort_tiles = cdiv(cap, kSortTile) + slots;
+  p.sort_tiles = cdiv(cap, kSortTileMin) + slots;  // room for the smallest tile
   p.flag_tiles = cdiv(cap, kFlagTile) + slots;
   p.groups = cdiv(cap, kWalkGroup) + slots;
   p.diag_chunks = cdiv(p.groups, kDiagChunk) + slots;
@@ -215,6 +215,8 @@ struct gs_ctx {
   uint32_t sel = 0;
   bool single = false;  // created by gs_create: one galaxy, node pool 2N + 4096
   int com_mode = kComF32;
+  int sort_items = kSortItems;     // tuning: keys per thread of a sort tile (8 or 16)
+  int walk_bps = kWalkBlocksPerSM; // tuning: persistent walk blocks per SM (1..8)
   bool walk_comp = false;  // Kahan-compensated far-field sums in the walk
   void* host_stage = nullptr;  // pinned: [slots] params
   std::map<int, cudaGraphExec_t> graphs;
@@ -405,7 +407,7 @@ int ensure_layout(gs_ctx* c) {
     d.diag_chunk0 = dc;
     h[r] = d;
     dc += cdiv(cdiv(s.n, kWalkGroup), kDiagChunk);
-    st += cdiv(s.n, kSortTile);
+    st += cdiv(s.n, (uint64_t)kSortThreads * c->sort_items);
     ft += cdiv(s.n, kFlagTile);
     gr += cdiv(s.n, kWalkGroup);
     hs = std::max(hs, order[r] + 1);
@@ -433,7 +435,7 @@ int ensure_layout(gs_ctx* c) {
   L.diag_chunks = dc;
   c->hist_slots = hs;
   c->seg_host = h;
-  c->walk_grid = std::min<uint32_t>(cdiv(gr, kWalkWarps), (uint32_t)c->sms * kWalkBlocksPerSM);
+  c->walk_grid = std::min<uint32_t>(cdiv(gr, kWalkWarps), (uint32_t)c->sms * c->walk_bps);
   c->drop_graphs();
   c->lay_dirty = false;
   return GS_OK;
@@ -452,9 +454,8 @@ void enqueue_codes_sort(gs_ctx* c, const float4* pos, uint32_t stride, int advan
                                                      kSortPasses);
 }
 
-// stable segmented sort of keys[0] -> keys[0] (sorted codes), vals[0] (gather
-// permutation) and, with inv, the inverse permutation.
-void enqueue_sort_passes(gs_ctx* c, bool inv) {
+template <int ITEMS>
+void sort_passes_items(gs_ctx* c, bool inv) {
   const Layout& L = c->lay;
   cudaStream_t s = c->stream;
   for (int p = 0; p < kSortPasses; p++) {
@@ -462,17 +463,24 @@ void enqueue_sort_passes(gs_ctx* c, bool inv) {
     uint32_t* lb = c->lookback() + (size_t)p * L.sort_tiles * 256;
     uint32_t* ctr = c->tile_ctr() + p;
     if (p == 0)
-      onesweep_pass<true, false><<<L.sort_tiles, kSortThreads, 0, s>>>(
+      onesweep_pass<true, false, ITEMS><<<L.sort_tiles, kSortThreads, 0, s>>>(
           c->keys[src], nullptr, c->keys[dst], c->vals[dst], nullptr, c->hist(), p, lb, ctr, L, c->st);
     else if (p < kSortPasses - 1)
-      onesweep_pass<false, false><<<L.sort_tiles, kSortThreads, 0, s>>>(
+      onesweep_pass<false, false, ITEMS><<<L.sort_tiles, kSortThreads, 0, s>>>(
           c->keys[src], c->vals[src], c->keys[dst], c->vals[dst], nullptr, c->hist(), p, lb, ctr, L,
           c->st);
     else
-      onesweep_pass<false, true><<<L.sort_tiles, kSortThreads, 0, s>>>(
+      onesweep_pass<false, true, ITEMS><<<L.sort_tiles, kSortThreads, 0, s>>>(
           c->keys[src], c->vals[src], c->keys[dst], c->vals[dst], inv ? c->inv : nullptr, c->hist(),
           p, lb, ctr, L, c->st);
   }
+}
+
+// stable segmented sort of keys[0] -> keys[0] (sorted codes), vals[0] (gather
+// permutation) and, with inv, the inverse permutation; tile size per the tuning.
+void enqueue_sort_passes(gs_ctx* c, bool inv) {
+  if (c->sort_items == 8) sort_passes_items<8>(c, inv);
+  else sort_passes_items<16>(c, inv);
 }
 
 // the trees over keys[0] (sorted codes) with COM from pos; root size from the
@@ -1140,6 +1148,33 @@ int gs_set_com_mode(gs_ctx* ctx, int mode) {
   if (mode != kComF32 && mode != kComF64) return ctx->fail(GS_EINVAL, "COM mode %d", mode);
   ctx->com_mode = mode;
   ctx->drop_graphs();
+  return GS_OK;
+}
+
+int gs_set_tuning(gs_ctx* ctx, int knob, int value) {
+  CTX_CHECK(ctx);
+  if (knob == GS_TUNE_WALK_BLOCKS_PER_SM) {
+    if (value < 1 || value > kWalkBlocksPerSM)
+      return ctx->fail(GS_EINVAL, "walk blocks per SM must be in [1, %d]", kWalkBlocksPerSM);
+    ctx->walk_bps = value;
+  } else if (knob == GS_TUNE_SORT_ITEMS) {
+    if (value != 8 && value != 16) return ctx->fail(GS_EINVAL, "sort keys per thread must be 8 or 16");
+    ctx->sort_items = value;
+  } else {
+    return ctx->fail(GS_EINVAL, "unknown tuning knob %d", knob);
+  }
+  CK(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+  ctx->lay_dirty = true;  // tiles and grid follow at the next step
+  ctx->drop_graphs();
+  return GS_OK;
+}
+
+int gs_get_tuning(gs_ctx* ctx, int knob, int* value) {
+  CTX_CHECK(ctx);
+  if (!value) return ctx->fail(GS_EINVAL, "value is NULL");
+  if (knob == GS_TUNE_WALK_BLOCKS_PER_SM) *value = ctx->walk_bps;
+  else if (knob == GS_TUNE_SORT_ITEMS) *value = ctx->sort_items;
+  else return ctx->fail(GS_EINVAL, "unknown tuning knob %d", knob);
   return GS_OK;
 }
 

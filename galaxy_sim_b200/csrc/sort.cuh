@@ -15,11 +15,9 @@ namespace gs {
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
-#ifndef GS_SORT_ITEMS
-#define GS_SORT_ITEMS 16
-#endif
-constexpr int kSortItems = GS_SORT_ITEMS;
-constexpr int kSortTile = kSortThreads * kSortItems;  // keys per tile
+constexpr int kSortItems = 16;                        // default keys per thread
+constexpr int kSortTile = kSortThreads * kSortItems;  // default keys per tile (4096)
+constexpr int kSortTileMin = kSortThreads * 8;        // smallest tile the runtime selects
 constexpr int kSortPasses = 4;                        // 30-bit codes, 8-bit digits
 constexpr uint32_t kLbAgg = 1u << 30;
 constexpr uint32_t kLbInc = 2u << 30;
@@ -44,12 +42,14 @@ __device__ inline void hist_add_warp(uint32_t* s_hist, uint32_t key, bool valid,
   }
 }
 
-// One digit pass over every galaxy of the layout. FIRST: payload = source index.
+// One digit pass over every galaxy of the layout, ITEMS keys per thread (tiles of
+// 256 x ITEMS keys; the layout's sort tiles must be cut to that size). FIRST:
+// payload = source index.
 // LAST: also writes the inverse permutation inv[payload] = destination when
 // inv_out is given (central-particle tracking).
 // hist: [slots][kSortPasses][256] digit counts of each galaxy; lookback: [sort tiles][256];
 // st: per-slot states (error word).
-template <bool FIRST, bool LAST>
+template <bool FIRST, bool LAST, int ITEMS = kSortItems>
 __global__ void __launch_bounds__(kSortThreads)
     onesweep_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                   uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
@@ -71,11 +71,12 @@ __global__ void __launch_bounds__(kSortThreads)
   DevState* sst = st + sd.slot;
   const uint32_t lt = tile - sd.sort_tile0;  // tile index within the galaxy
   const uint32_t seg_end = sd.off + sd.n;
-  const uint32_t base = sd.off + lt * kSortTile + warp * (kSortTile / kSortWarps);
+  constexpr int kTileKeys = kSortThreads * ITEMS;
+  const uint32_t base = sd.off + lt * kTileKeys + warp * (kTileKeys / kSortWarps);
 
-  uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+  uint32_t key[ITEMS], val[ITEMS], rank[ITEMS];
 #pragma unroll
-  for (int k = 0; k < kSortItems; k++) {
+  for (int k = 0; k < ITEMS; k++) {
     const uint32_t idx = base + k * 32 + lane;
     if (idx < seg_end) {
       key[k] = keys_in[idx];
@@ -87,7 +88,7 @@ __global__ void __launch_bounds__(kSortThreads)
   }
   const unsigned lt_mask = (1u << lane) - 1u;
 #pragma unroll
-  for (int k = 0; k < kSortItems; k++) {
+  for (int k = 0; k < ITEMS; k++) {
     const bool valid = base + k * 32 + lane < seg_end;
     const uint32_t d = (key[k] >> shift) & 255u;
     const unsigned peers = __match_any_sync(0xffffffffu, valid ? d : 0x100u + lane);
@@ -166,7 +167,7 @@ __global__ void __launch_bounds__(kSortThreads)
   __syncthreads();
 
 #pragma unroll
-  for (int k = 0; k < kSortItems; k++) {
+  for (int k = 0; k < ITEMS; k++) {
     if (base + k * 32 + lane < seg_end) {
       const uint32_t dd = (key[k] >> shift) & 255u;
       const uint32_t pos = s_prefix[dd] + s_warp[warp][dd] + rank[k];

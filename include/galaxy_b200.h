@@ -113,6 +113,14 @@ int gs_set_star_formation(gs_ctx* ctx, int enable);
  * contributions summed with Kahan compensation. Together with gs_set_com_mode
  * this selects the precision variant; no counterpart in the reference. */
 int gs_set_walk_mode(gs_ctx* ctx, int compensated);
+/* Launch tuning that never changes results (no counterpart in the reference):
+ * GS_TUNE_WALK_BLOCKS_PER_SM = persistent walk blocks per SM (1..8, default 8),
+ * GS_TUNE_SORT_ITEMS = keys per thread of a sort tile (8 or 16, default 16). Takes
+ * effect at the next step; galaxy_sim_b200/autotune.py picks values by timing. */
+#define GS_TUNE_WALK_BLOCKS_PER_SM 1
+#define GS_TUNE_SORT_ITEMS 2
+int gs_set_tuning(gs_ctx* ctx, int knob, int value);
+int gs_get_tuning(gs_ctx* ctx, int knob, int* value);
 /* NBodyGPU.updateCentralMass (NBodyGPU.js:245-251): both ping-pong buffers. */
 int gs_update_central_mass(gs_ctx* ctx, float mass, uint32_t idx);
 /* NBodyGPU.applyPermutation (NBodyGPU.js:225-238): gather out[i] = in[perm[i]] of
