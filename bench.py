@@ -91,6 +91,22 @@ def init_dist(ws, backend):
     return dist
 
 
+def rank_max(dist, ms: float, device: str) -> float:
+    """The slowest rank's device time: every rank contributes its own ms, all get
+    the maximum (one all-reduce, the same call on every rank)."""
+    import torch
+
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(units_per_rank: float, ws: int, max_ms: float) -> float:
+    """Whole-job throughput of ws replicas: all ranks' units over the slowest rank's time."""
+    return units_per_rank * ws / (max_ms / 1e3)
+
+
 def workload(args):
     from galaxy_sim_b200 import simulation as S
 
@@ -211,11 +227,8 @@ def run_ours(args, ws, rank, local):
     errs = sim.gpu.deviceErrors()
     if errs:
         raise RuntimeError(f"device error word 0x{errs:x} during the timed steps")
-    t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
-    value = N * K * ws / (max_ms / 1e3)
+    max_ms = rank_max(dist, total_ms, f"cuda:{local}")
+    value = job_value(N * K, ws, max_ms)
     clocks = clk.summary()
 
     # ---- walk kernel, timed alone on the same stream (roofline of the dominant kernel) ----
@@ -292,13 +305,10 @@ def run_ours(args, ws, rank, local):
         with torch.cuda.stream(ext):
             e1.record(ext)
         torch.cuda.synchronize()
-        te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f"cuda:{local}")
-        if dist:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        te_ms = float(te.item())
+        te_ms = rank_max(dist, e0.elapsed_time(e1), f"cuda:{local}")
         if not np.isfinite(diag.e_diag):
             raise RuntimeError("non-finite energy diagnostic in the e2e run")
-        e2e = {"value": round(N * Ke * ws / (te_ms / 1e3), 1), "unit": UNIT,
+        e2e = {"value": round(job_value(N * Ke, ws, te_ms), 1), "unit": UNIT,
                "h2d_bytes_per_step": int(round((N * 48 + Ke * 96) / Ke)),
                "d2h_bytes_per_step": int(round((Ke * 48 + N * 48) / Ke)),
                "path": "gs_write_state (pinned) + K x [gs_update_params, gs_run(1), gs_energy] "
