@@ -643,13 +643,18 @@ int wait_stream(gs_ctx* c, uint64_t timeout_ns, const Slot* s) {
       std::this_thread::sleep_for(std::chrono::microseconds(50));
     }
   }
-  // error words: the given slot's, or every live slot's
+  // error words: the given slot's, or every live slot's (one strided copy)
   unsigned err = 0;
-  for (uint32_t k = 0; k < c->slots.size(); k++) {
-    if (s ? (&c->slots[k] != s) : !c->slots[k].live) continue;
-    unsigned e = 0;
-    CK(c, cudaMemcpy(&e, &c->st[k].err, sizeof(unsigned), cudaMemcpyDeviceToHost), "read error word");
-    err |= e;
+  if (s) {
+    const size_t k = (size_t)(s - c->slots.data());
+    CK(c, cudaMemcpy(&err, &c->st[k].err, sizeof(unsigned), cudaMemcpyDeviceToHost), "read error word");
+  } else if (!c->slots.empty()) {
+    std::vector<unsigned> words(c->slots.size());
+    CK(c, cudaMemcpy2D(words.data(), sizeof(unsigned), &c->st[0].err, sizeof(DevState), sizeof(unsigned),
+                       c->slots.size(), cudaMemcpyDeviceToHost),
+       "read error words");
+    for (size_t k = 0; k < words.size(); k++)
+      if (c->slots[k].live) err |= words[k];
   }
   if (err)
     return c->fail(GS_EDEVICE, "device error word 0x%x (%s%s%s%s)", err,
