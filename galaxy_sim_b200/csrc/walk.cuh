@@ -31,7 +31,7 @@ namespace gs {
 constexpr int kWalkThreads = 128;
 constexpr int kWalkWarps = kWalkThreads / 32;
 constexpr int kPartials = 6;  // e_diag, e_true, px, py, pz, mass
-constexpr int kWalkStack = 96;  // ranges; a range push per opened node, <= 7 * depth + 1
+constexpr int kWalkStack = 192;  // ranges; two pops per round explore two paths, each <= 7 per depth
 #ifndef GS_WALK_BLOCKS_PER_SM
 #define GS_WALK_BLOCKS_PER_SM 8
 #endif
@@ -112,8 +112,8 @@ struct WalkArgs {
 // Per-warp shared staging.
 struct WalkSmem {
   uint2 stack[kWalkStack];          // {first child | (count-1) << 29, lane mask}
-  float cx[8], cy[8], cz[8], cmass[8], cs2[8];
-  uint4 cmeta[8];                   // {child, info, own-leaf density bits, massive}
+  float cx[16], cy[16], cz[16], cmass[16], cs2[16];  // two staged child ranges
+  uint4 cmeta[16];                  // {child, info, own-leaf density bits, massive}
   float lx[66], ly[66], lz[66], lm[66];
   uint4 bl[4];                      // leaf batch: {first particle, count, lane mask, 0}
 };
@@ -238,34 +238,43 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
     uint32_t budget = 4u * sd.node_cap + 1024u;
     while (sp > 0) {
       __syncwarp();
-      const uint2 e = S.stack[--sp];
-      const uint32_t start = e.x & 0x1fffffffu;
-      const uint32_t cnt = (e.x >> 29) + 1u;
-      const unsigned mask = e.y;
+      // pop up to two ranges; their children are staged and tested together
+      const bool two = sp >= 2;
+      const uint2 e0 = S.stack[sp - 1];
+      const uint2 e1 = two ? S.stack[sp - 2] : make_uint2(0u, 0u);
+      sp -= two ? 2 : 1;
+      const uint32_t start0 = e0.x & 0x1fffffffu, cnt0 = (e0.x >> 29) + 1u;
+      const uint32_t start1 = e1.x & 0x1fffffffu, cnt1 = two ? (e1.x >> 29) + 1u : 0u;
+      const unsigned mask0 = e0.y, mask1 = e1.y;
       if (--budget == 0) {
         if (lane == 0) raise_err(sst, GS_DERR_STACK);
         break;
       }
       __syncwarp();
-      // Stage the range in lanes 0..7: one child per lane; lanes past the count hold
-      // massless dummies. Massless and sub-softening children (size^2 < eps^2/4,
-      // always accepted, nbody_bh.wgsl:112) get size^2 = -inf, so the per-lane test
-      // is the single compare size^2 < theta^2 (r^2 + eps^2).
-      bool own = false;
-      if (lane < 8) {
+      // Stage range 0 in lanes 0..7 and range 1 in lanes 8..15: one child per lane;
+      // slots past a range's count hold massless dummies. Massless and sub-softening
+      // children (size^2 < eps^2/4, always accepted, nbody_bh.wgsl:112) get
+      // size^2 = -inf, so the per-lane test is the single compare size^2 < theta^2 (r^2 + eps^2).
+      bool own = false, isleaf = false, massive = false;
+      if (lane < 16) {
+        const uint32_t rc = lane < 8 ? cnt0 : cnt1;
+        const uint32_t rs = lane < 8 ? start0 : start1;
+        const uint32_t c = lane & 7;
         float4 q = make_float4(1e30f, 1e30f, 1e30f, 0.f);
         WalkInfo w;
         w.s2 = 0.f;
         w.child = 0;
         w.info = kLeafBit;
         w.size = 1.f;
-        if (lane < (int)cnt) {
-          q = __ldg(&a.cm[start + lane]);
-          w = a.info[start + lane];
+        const bool real = c < rc;
+        if (real) {
+          q = __ldg(&a.cm[rs + c]);
+          w = a.info[rs + c];
         }
         const uint32_t wc = w.info & ~kLeafBit;
-        own = lane < (int)cnt && (w.info & kLeafBit) && q.w != 0.0f && w.child < gend &&
-              w.child + wc > gbeg;
+        isleaf = real && (w.info & kLeafBit);
+        massive = real && q.w != 0.0f;
+        own = isleaf && q.w != 0.0f && w.child < gend && w.child + wc > gbeg;
         float s2 = w.s2;
         if (q.w == 0.0f) {  // never opened, contributes nothing (far away, massless)
           s2 = -INFINITY;
@@ -280,18 +289,20 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
         S.cs2[lane] = s2;
         S.cmeta[lane] = make_uint4(w.child, w.info,
                                    own ? __float_as_uint((float)wc / (w.size * w.size * w.size)) : 0u,
-                                   q.w != 0.0f ? 1u : 0u);
+                                   massive ? 1u : 0u);
       }
-      const unsigned ownmask = __ballot_sync(full, own) & 0xffu;  // leaves holding our particles
-      const unsigned leafmask = __ballot_sync(full, lane < (int)cnt && (S.cmeta[lane & 7].y & kLeafBit)) & 0xffu;
-      const unsigned massmask = DBG ? (__ballot_sync(full, lane < (int)cnt && S.cmeta[lane & 7].w) & 0xffu) : 0u;
+      const unsigned ownmask = __ballot_sync(full, own);  // leaves holding our particles
+      const unsigned leafmask = __ballot_sync(full, isleaf);
+      const unsigned massmask = DBG ? __ballot_sync(full, massive) : 0u;
       __syncwarp();
-      const bool act = (mask >> lane) & 1u;
-      const float2 actw = f2(act ? 1.0f : 0.0f);
-      float2 wt[4];  // accept weights (1.0 / 0.0) of children 2p, 2p+1
+      const bool act0 = (mask0 >> lane) & 1u, act1 = (mask1 >> lane) & 1u;
+      uint32_t obits = 0;  // children this lane opens (active, accept weight 0), bit = slot
+      const int npairs = two ? 8 : 4;
 #pragma unroll
-      for (int pp = 0; pp < 4; pp++) {
+      for (int pp = 0; pp < 8; pp++) {
+        if (pp >= npairs) break;
         const int c = 2 * pp;
+        const float2 actw = f2((pp < 4 ? act0 : act1) ? 1.0f : 0.0f);
         const float2 qx = *reinterpret_cast<const float2*>(&S.cx[c]);
         const float2 qy = *reinterpret_cast<const float2*>(&S.cy[c]);
         const float2 qz = *reinterpret_cast<const float2*>(&S.cz[c]);
@@ -301,7 +312,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
         const float2 d2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __ffma2_rn(rz, rz, f2(eps2))));
         const float2 td = __fmul2_rn(f2(theta2), d2);
         const float2 w = __fmul2_rn(make_float2(set_gt(td.x, s2.x), set_gt(td.y, s2.y)), actw);
-        wt[pp] = w;
+        obits |= ((w.x == 0.0f ? 1u : 0u) | (w.y == 0.0f ? 2u : 0u)) << c;
         const float2 rinv = __fmul2_rn(make_float2(rsqrtf(d2.x), rsqrtf(d2.y)), w);
         const float2 mr = __fmul2_rn(qm, rinv);
         const float2 f = __fmul2_rn(__fmul2_rn(mr, rinv), rinv);
@@ -317,23 +328,25 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
           pt = __fadd2_rn(pt, mr);  // sum of m/r; potential = -G * sum
         }
       }
-      // bitmask of the children this lane opens (active, accept weight 0)
-      uint32_t obits = 0;
-#pragma unroll
-      for (int pp = 0; pp < 4; pp++) {
-        obits |= (wt[pp].x == 0.0f ? 1u : 0u) << (2 * pp);
-        obits |= (wt[pp].y == 0.0f ? 1u : 0u) << (2 * pp + 1);
-      }
-      obits = act ? (obits & ((1u << cnt) - 1u)) : 0u;
+      const uint32_t cm0 = (1u << cnt0) - 1u, cm1 = ((1u << cnt1) - 1u) << 8;
+      obits &= (act0 ? cm0 : 0u) | (act1 ? cm1 : 0u);
       const uint32_t om = __reduce_or_sync(full, obits);  // children opened by some lane
-      if (DBG && act) {
-        const uint32_t real = __popc(massmask & ((1u << cnt) - 1u));
-        nvisit += real;
-        nmono += real - __popc(obits);
+      if (DBG) {
+        if (act0) {
+          const uint32_t real = __popc(massmask & cm0);
+          nvisit += real;
+          nmono += real - __popc(obits & cm0);
+        }
+        if (act1) {
+          const uint32_t real = __popc(massmask & cm1);
+          nvisit += real;
+          nmono += real - __popc(obits & cm1);
+        }
       }
       for (uint32_t bb = ownmask; bb; bb &= bb - 1) {  // own-leaf density (nbody_bh.wgsl:93-95)
-        const uint4 mt = S.cmeta[__ffs(bb) - 1];
-        if (act && (i - mt.x) < (mt.y & ~kLeafBit)) dens = __uint_as_float(mt.z);
+        const uint32_t cc = __ffs(bb) - 1;
+        const uint4 mt = S.cmeta[cc];
+        if ((cc < 8 ? act0 : act1) && (i - mt.x) < (mt.y & ~kLeafBit)) dens = __uint_as_float(mt.z);
       }
       if (!om) continue;
       // opened internal children: push their child ranges
@@ -342,9 +355,10 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
         const unsigned open = __ballot_sync(full, (obits >> cc) & 1u);
         const uint4 mt = S.cmeta[cc];
         const uint32_t cchild = mt.x, ccnt = mt.y & ~kLeafBit;
+        const uint32_t self = (cc < 8 ? start0 : start1) + (cc & 7);
         // a galaxy's child ranges stay in its node range by construction (build,
         // upload check); the walk itself only guards the pool bounds
-        if (!(cchild > start + cc && (uint64_t)cchild + ccnt <= a.node_pool && ccnt >= 1u && ccnt <= 8u)) {
+        if (!(cchild > self && (uint64_t)cchild + ccnt <= a.node_pool && ccnt >= 1u && ccnt <= 8u)) {
           if (lane == 0) raise_err(sst, GS_DERR_TREE);
           continue;
         }
