@@ -31,7 +31,12 @@ namespace gs {
 constexpr int kWalkThreads = 128;
 constexpr int kWalkWarps = kWalkThreads / 32;
 constexpr int kPartials = 6;  // e_diag, e_true, px, py, pz, mass
-constexpr int kWalkStack = 192;  // ranges; two pops per round explore two paths, each <= 7 per depth
+#ifndef GS_WALK_RANGES
+#define GS_WALK_RANGES 4
+#endif
+constexpr int kWalkRanges = GS_WALK_RANGES;  // child ranges popped and tested per round (1..4)
+// ranges; a round explores kWalkRanges paths, each leaving <= 7 pending ranges per depth
+constexpr int kWalkStack = 8 * 11 * kWalkRanges;
 #ifndef GS_WALK_BLOCKS_PER_SM
 #define GS_WALK_BLOCKS_PER_SM 8
 #endif
@@ -112,8 +117,10 @@ struct WalkArgs {
 // Per-warp shared staging.
 struct WalkSmem {
   uint2 stack[kWalkStack];          // {first child | (count-1) << 29, lane mask}
-  float cx[16], cy[16], cz[16], cmass[16], cs2[16];  // two staged child ranges
-  uint4 cmeta[16];                  // {child, info, own-leaf density bits, massive}
+  float cx[8 * kWalkRanges], cy[8 * kWalkRanges], cz[8 * kWalkRanges];  // staged child ranges
+  float cmass[8 * kWalkRanges], cs2[8 * kWalkRanges];
+  uint32_t cnode[8 * kWalkRanges];  // node index of each staged child
+  uint4 cmeta[8 * kWalkRanges];     // {child, info, own-leaf density bits, massive}
   float lx[66], ly[66], lz[66], lm[66];
   uint4 bl[4];                      // leaf batch: {first particle, count, lane mask, 0}
 };
@@ -238,28 +245,32 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
     uint32_t budget = 4u * sd.node_cap + 1024u;
     while (sp > 0) {
       __syncwarp();
-      // pop up to two ranges; their children are staged and tested together
-      const bool two = sp >= 2;
-      const uint2 e0 = S.stack[sp - 1];
-      const uint2 e1 = two ? S.stack[sp - 2] : make_uint2(0u, 0u);
-      sp -= two ? 2 : 1;
-      const uint32_t start0 = e0.x & 0x1fffffffu, cnt0 = (e0.x >> 29) + 1u;
-      const uint32_t start1 = e1.x & 0x1fffffffu, cnt1 = two ? (e1.x >> 29) + 1u : 0u;
-      const unsigned mask0 = e0.y, mask1 = e1.y;
+      // pop up to kWalkRanges ranges; their children are staged and tested together
+      const int nr = min(sp, kWalkRanges);
+      const int sp0 = sp;
+      sp -= nr;
+      uint32_t masks[kWalkRanges];
+      uint32_t cnts = 0;  // 4 bits per range
+#pragma unroll
+      for (int r = 0; r < kWalkRanges; r++) {
+        const uint2 e = r < nr ? S.stack[sp0 - 1 - r] : make_uint2(0u, 0u);
+        masks[r] = e.y;
+        cnts |= (r < nr ? (e.x >> 29) + 1u : 0u) << (4 * r);
+      }
       if (--budget == 0) {
         if (lane == 0) raise_err(sst, GS_DERR_STACK);
         break;
       }
-      __syncwarp();
-      // Stage range 0 in lanes 0..7 and range 1 in lanes 8..15: one child per lane;
-      // slots past a range's count hold massless dummies. Massless and sub-softening
-      // children (size^2 < eps^2/4, always accepted, nbody_bh.wgsl:112) get
-      // size^2 = -inf, so the per-lane test is the single compare size^2 < theta^2 (r^2 + eps^2).
+      // Stage range r in lanes 8r..8r+7: one child per lane; slots past a range's
+      // count hold massless dummies. Massless and sub-softening children
+      // (size^2 < eps^2/4, always accepted, nbody_bh.wgsl:112) get size^2 = -inf,
+      // so the per-lane test is the single compare size^2 < theta^2 (r^2 + eps^2).
       bool own = false, isleaf = false, massive = false;
-      if (lane < 16) {
-        const uint32_t rc = lane < 8 ? cnt0 : cnt1;
-        const uint32_t rs = lane < 8 ? start0 : start1;
+      if (lane < 8 * kWalkRanges) {
+        const int r = lane >> 3;
         const uint32_t c = lane & 7;
+        const uint2 e = r < nr ? S.stack[sp0 - 1 - r] : make_uint2(0u, 0u);
+        const uint32_t rs = e.x & 0x1fffffffu, rc = r < nr ? (e.x >> 29) + 1u : 0u;
         float4 q = make_float4(1e30f, 1e30f, 1e30f, 0.f);
         WalkInfo w;
         w.s2 = 0.f;
@@ -287,6 +298,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
         S.cz[lane] = q.z;
         S.cmass[lane] = q.w;
         S.cs2[lane] = s2;
+        S.cnode[lane] = rs + c;
         S.cmeta[lane] = make_uint4(w.child, w.info,
                                    own ? __float_as_uint((float)wc / (w.size * w.size * w.size)) : 0u,
                                    massive ? 1u : 0u);
@@ -295,14 +307,20 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
       const unsigned leafmask = __ballot_sync(full, isleaf);
       const unsigned massmask = DBG ? __ballot_sync(full, massive) : 0u;
       __syncwarp();
-      const bool act0 = (mask0 >> lane) & 1u, act1 = (mask1 >> lane) & 1u;
-      uint32_t obits = 0;  // children this lane opens (active, accept weight 0), bit = slot
-      const int npairs = two ? 8 : 4;
+      uint32_t actbits = 0, keep = 0;  // per range: this lane active; slots this lane may open
 #pragma unroll
-      for (int pp = 0; pp < 8; pp++) {
-        if (pp >= npairs) break;
+      for (int r = 0; r < kWalkRanges; r++) {
+        const uint32_t a_r = (masks[r] >> lane) & 1u;
+        actbits |= a_r << r;
+        const uint32_t cr = (cnts >> (4 * r)) & 15u;
+        keep |= a_r ? ((1u << cr) - 1u) << (8 * r) : 0u;
+      }
+      uint32_t obits = 0;  // children this lane opens (active, accept weight 0), bit = slot
+#pragma unroll
+      for (int pp = 0; pp < 4 * kWalkRanges; pp++) {
+        if (pp >= 4 * nr) break;
         const int c = 2 * pp;
-        const float2 actw = f2((pp < 4 ? act0 : act1) ? 1.0f : 0.0f);
+        const float2 actw = f2((actbits >> (pp >> 2)) & 1u ? 1.0f : 0.0f);
         const float2 qx = *reinterpret_cast<const float2*>(&S.cx[c]);
         const float2 qy = *reinterpret_cast<const float2*>(&S.cy[c]);
         const float2 qz = *reinterpret_cast<const float2*>(&S.cz[c]);
@@ -328,25 +346,17 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
           pt = __fadd2_rn(pt, mr);  // sum of m/r; potential = -G * sum
         }
       }
-      const uint32_t cm0 = (1u << cnt0) - 1u, cm1 = ((1u << cnt1) - 1u) << 8;
-      obits &= (act0 ? cm0 : 0u) | (act1 ? cm1 : 0u);
+      obits &= keep;
       const uint32_t om = __reduce_or_sync(full, obits);  // children opened by some lane
       if (DBG) {
-        if (act0) {
-          const uint32_t real = __popc(massmask & cm0);
-          nvisit += real;
-          nmono += real - __popc(obits & cm0);
-        }
-        if (act1) {
-          const uint32_t real = __popc(massmask & cm1);
-          nvisit += real;
-          nmono += real - __popc(obits & cm1);
-        }
+        const uint32_t real = __popc(massmask & keep);
+        nvisit += real;
+        nmono += real - __popc(obits);
       }
       for (uint32_t bb = ownmask; bb; bb &= bb - 1) {  // own-leaf density (nbody_bh.wgsl:93-95)
         const uint32_t cc = __ffs(bb) - 1;
         const uint4 mt = S.cmeta[cc];
-        if ((cc < 8 ? act0 : act1) && (i - mt.x) < (mt.y & ~kLeafBit)) dens = __uint_as_float(mt.z);
+        if (((actbits >> (cc >> 3)) & 1u) && (i - mt.x) < (mt.y & ~kLeafBit)) dens = __uint_as_float(mt.z);
       }
       if (!om) continue;
       // opened internal children: push their child ranges
@@ -355,10 +365,9 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
         const unsigned open = __ballot_sync(full, (obits >> cc) & 1u);
         const uint4 mt = S.cmeta[cc];
         const uint32_t cchild = mt.x, ccnt = mt.y & ~kLeafBit;
-        const uint32_t self = (cc < 8 ? start0 : start1) + (cc & 7);
         // a galaxy's child ranges stay in its node range by construction (build,
         // upload check); the walk itself only guards the pool bounds
-        if (!(cchild > self && (uint64_t)cchild + ccnt <= a.node_pool && ccnt >= 1u && ccnt <= 8u)) {
+        if (!(cchild > S.cnode[cc] && (uint64_t)cchild + ccnt <= a.node_pool && ccnt >= 1u && ccnt <= 8u)) {
           if (lane == 0) raise_err(sst, GS_DERR_TREE);
           continue;
         }
