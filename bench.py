@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched/served comparison")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch knobs")
     ap.add_argument("--requests", type=int, default=16, help="serve: requests in the stream")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrival rate (1/s)")
     ap.add_argument("--min-steps", type=int, default=100, help="serve: fewest steps of a request")
@@ -200,7 +201,9 @@ def run_ours(args, ws, rank, local):
     # launch knobs (walk grid, sort tile) timed on this workload; results do not depend on them
     from galaxy_sim_b200.autotune import autotune
 
-    tuned = autotune(sim.gpu, steps=5, warmup=2, star_formation=sim.star_formation, device=local)
+    tuned = None
+    if not args.no_tune:
+        tuned = autotune(sim.gpu, steps=5, warmup=2, star_formation=sim.star_formation, device=local)
     sim.run(args.warmup)
     sim.sync()
     # kernels per step, counted from the captured step graph: bbox, codes, 4 sort
