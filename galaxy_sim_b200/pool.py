@@ -149,6 +149,51 @@ class GalaxyPool:
         self._ok(lib().gs_device_errors(self._ctx, C.byref(b), int(bool(clear))))
         return b.value
 
+    # -- the NBodyGPU surface on one slot ------------------------------------------------------
+    def apply_permutation(self, slot: int, perm):
+        """NBodyGPU.applyPermutation on one galaxy (out[i] = in[perm[i]], galaxy-local)."""
+        self._sel(slot)
+        p = np.ascontiguousarray(perm, np.uint32)
+        if p.size != self.n[slot]:
+            raise ValueError("perm must hold N indices")
+        self._ok(lib().gs_apply_permutation(self._ctx, ptr(p)))
+
+    def upload_tree(self, slot: int, nodes, num_nodes: int, level_ranges=None):
+        """NBodyGPU.uploadBHTree on one galaxy (BHNode array with galaxy-local indices)."""
+        self._sel(slot)
+        nd = np.ascontiguousarray(nodes).view(np.uint8)
+        lr, nl = None, 0
+        if level_ranges is not None:
+            lr = np.ascontiguousarray(np.asarray(level_ranges, np.uint32).reshape(-1, 2)[:16])
+            nl = lr.shape[0]
+        self._ok(lib().gs_upload_tree(self._ctx, ptr(nd), int(num_nodes), ptr(lr), nl))
+
+    def get_tree(self, slot: int, want_perm: bool = True):
+        """(nodes, level ranges, permutation of the last rebuild) of one galaxy."""
+        from ._lib import NODE_DTYPE
+
+        self._sel(slot)
+        nn, nl = C.c_uint32(0), C.c_uint32(0)
+        self._ok(lib().gs_get_tree(self._ctx, None, 0, C.byref(nn), None, 0, C.byref(nl), None))
+        nodes = np.zeros(max(nn.value, 1), NODE_DTYPE)
+        lr = np.zeros(2 * max(nl.value, 1), np.uint32)
+        perm = np.zeros(self.n[slot], np.uint32) if want_perm else None
+        self._ok(lib().gs_get_tree(self._ctx, ptr(nodes), nn.value, C.byref(nn), ptr(lr), nl.value,
+                                   C.byref(nl), ptr(perm)))
+        return nodes[: nn.value], lr[: 2 * nl.value].reshape(-1, 2), perm
+
+    def refresh(self):
+        """NBodyGPU.encodeRefresh for every resident galaxy."""
+        self._ok(lib().gs_refresh(self._ctx))
+
+    def step(self):
+        """NBodyGPU.step (walk + halo + kick-drift) for every resident galaxy."""
+        self._ok(lib().gs_step(self._ctx))
+
+    def sort_build(self):
+        """The on-device rebuild for every resident galaxy."""
+        self._ok(lib().gs_sort_build(self._ctx))
+
     # -- stepping --------------------------------------------------------------------------
     def run(self, nsteps: int, star_formation: bool = False):
         self._ok(lib().gs_run(self._ctx, int(nsteps), int(bool(star_formation))))
