@@ -12,9 +12,10 @@
 // only if it opened every ancestor), so the per-particle interaction set equals
 // the reference's thread-per-particle stack walk.
 //   * The stack holds child ranges (children of a BFS node are contiguous) with
-//     the mask of lanes that opened the parent; a popped range is staged into
-//     shared memory by one coalesced load (one child per lane) in
-//     structure-of-arrays form.
+//     the mask of lanes that opened the parent. Each round pops up to four
+//     ranges and stages their children into shared memory by one coalesced load
+//     (one child per lane, structure of arrays), so the round's stack, ballot and
+//     staging work is shared by up to 32 children.
 //   * Children are tested two at a time, and an opened leaf's particles are
 //     staged the same way and summed two at a time, with sm_100's packed
 //     FP32x2 FMA/ADD/MUL; accumulation is predicated, not branched.
