@@ -62,6 +62,7 @@ struct BuildBuffers {
 
 // K1: per particle D, L and per-tile start counts.
 __global__ void __launch_bounds__(kFlagThreads) tree_flags_kernel(BuildBuffers b, Layout Lo) {
+  griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
   __shared__ uint32_t s_code[kFlagTile + 32];
   __shared__ int8_t s_cpd16[kFlagTile + 16];
   __shared__ uint32_t s_red[kFlagThreads / 32][kCounters];
@@ -137,6 +138,7 @@ constexpr int kScanThreads = 1024;
 __global__ void __launch_bounds__(kScanThreads)
     tree_scan_kernel(BuildBuffers b, Layout Lo, double root_size, const MortonFrame* frames,
                      DevState* st) {
+  griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
   __shared__ uint32_t s_warp[kScanThreads / 32][kCounters];
   __shared__ uint32_t s_tot[kCounters];
   const uint32_t seg = blockIdx.x;
@@ -207,6 +209,7 @@ __global__ void __launch_bounds__(kScanThreads)
 // K3: node indices, parents, child bases, leaf lists.
 __global__ void __launch_bounds__(kFlagThreads) tree_emit_kernel(BuildBuffers b, Layout Lo,
                                                                   DevState* st) {
+  griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
   __shared__ uint32_t s_warp[kFlagThreads / 32][kCounters];
   __shared__ TreeMeta s_meta;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -314,6 +317,7 @@ template <int MODE>
 __global__ void __launch_bounds__(kLeafThreads)
     tree_leaves_kernel(BuildBuffers b, Layout Lo, const float4* __restrict__ pos,
                        uint32_t pos_stride, DevState* st) {
+  griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
   do {  // `continue` leaves the block's single iteration
     const uint32_t tile = blockIdx.x;
     const SegDesc sd = Lo.segs[Lo.seg_of_flag_tile[tile]];

@@ -81,4 +81,10 @@ __device__ inline float ordered_to_float(int i) {
 
 __device__ inline void raise_err(DevState* st, unsigned bits) { atomicOr(&st->err, bits); }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may start while its predecessor drains; it waits here, before
+// touching any memory, until the predecessor grids have completed and flushed.
+// Without such a dependency the wait returns at once.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 }  // namespace gs

@@ -52,6 +52,23 @@ void set_err(char* dst, const char* fmt, ...) {
   va_end(ap);
 }
 
+// Launch with programmatic stream serialization: the kernel may be scheduled
+// while its predecessor in the stream drains and waits for it in griddep_wait().
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 uint32_t grid_for(uint64_t N, uint32_t threads, uint32_t cap_blocks) {
   return std::min<uint32_t>(cap_blocks, std::max<uint32_t>(1, cdiv(N, threads)));
 }
@@ -446,12 +463,12 @@ int ensure_layout(gs_ctx* c) {
 void enqueue_codes_sort(gs_ctx* c, const float4* pos, uint32_t stride, int advance_time) {
   const Layout& L = c->lay;
   cudaStream_t s = c->stream;
-  bbox_kernel<<<L.flag_tiles, kTileThreads, 0, s>>>(pos, stride, L, c->bbox_part, c->seg_ctr,
-                                                    c->frames, c->st, advance_time);
-  cudaMemsetAsync(c->sort_scratch, 0, sizeof(uint32_t) * (size_t)c->hist_slots * kSortPasses * 256, s);
-  cudaMemsetAsync(c->tile_ctr(), 0, sizeof(uint32_t) * (16 + (size_t)kSortPasses * L.sort_tiles * 256), s);
-  codes_kernel<<<L.flag_tiles, kTileThreads, 0, s>>>(pos, stride, L, c->frames, c->keys[0], c->hist(),
-                                                     kSortPasses);
+  launch_pdl(bbox_kernel, L.flag_tiles, kTileThreads, s, pos, stride, L, c->bbox_part, c->seg_ctr,
+             c->frames, c->st, advance_time, c->sort_scratch,
+             (uint32_t)((size_t)c->hist_slots * kSortPasses * 256), c->tile_ctr(),
+             (uint32_t)(16 + (size_t)kSortPasses * L.sort_tiles * 256));
+  launch_pdl(codes_kernel, L.flag_tiles, kTileThreads, s, pos, stride, L, (const MortonFrame*)c->frames,
+             c->keys[0], c->hist(), (int)kSortPasses);
 }
 
 template <int ITEMS>
@@ -462,17 +479,19 @@ void sort_passes_items(gs_ctx* c, bool inv) {
     const int src = p & 1, dst = src ^ 1;
     uint32_t* lb = c->lookback() + (size_t)p * L.sort_tiles * 256;
     uint32_t* ctr = c->tile_ctr() + p;
+    const uint32_t* kin = c->keys[src];
+    const uint32_t* vin = p == 0 ? nullptr : c->vals[src];
+    uint32_t* iv = (p == kSortPasses - 1 && inv) ? c->inv : nullptr;
+    const uint32_t* h = c->hist();
     if (p == 0)
-      onesweep_pass<true, false, ITEMS><<<L.sort_tiles, kSortThreads, 0, s>>>(
-          c->keys[src], nullptr, c->keys[dst], c->vals[dst], nullptr, c->hist(), p, lb, ctr, L, c->st);
+      launch_pdl(onesweep_pass<true, false, ITEMS>, L.sort_tiles, kSortThreads, s, kin, vin, c->keys[dst],
+                 c->vals[dst], iv, h, p, lb, ctr, L, c->st);
     else if (p < kSortPasses - 1)
-      onesweep_pass<false, false, ITEMS><<<L.sort_tiles, kSortThreads, 0, s>>>(
-          c->keys[src], c->vals[src], c->keys[dst], c->vals[dst], nullptr, c->hist(), p, lb, ctr, L,
-          c->st);
+      launch_pdl(onesweep_pass<false, false, ITEMS>, L.sort_tiles, kSortThreads, s, kin, vin, c->keys[dst],
+                 c->vals[dst], iv, h, p, lb, ctr, L, c->st);
     else
-      onesweep_pass<false, true, ITEMS><<<L.sort_tiles, kSortThreads, 0, s>>>(
-          c->keys[src], c->vals[src], c->keys[dst], c->vals[dst], inv ? c->inv : nullptr, c->hist(),
-          p, lb, ctr, L, c->st);
+      launch_pdl(onesweep_pass<false, true, ITEMS>, L.sort_tiles, kSortThreads, s, kin, vin, c->keys[dst],
+                 c->vals[dst], iv, h, p, lb, ctr, L, c->st);
   }
 }
 
@@ -490,15 +509,15 @@ void enqueue_build(gs_ctx* c, const float4* pos, uint32_t stride, int com_mode, 
   const Layout& L = c->lay;
   cudaStream_t s = c->stream;
   BuildBuffers b = c->bb();
-  tree_flags_kernel<<<L.flag_tiles, kFlagThreads, 0, s>>>(b, L);
-  tree_scan_kernel<<<L.nseg, kScanThreads, 0, s>>>(b, L, root_size, frames, c->st);
-  tree_emit_kernel<<<L.flag_tiles, kFlagThreads, 0, s>>>(b, L, c->st);
+  launch_pdl(tree_flags_kernel, L.flag_tiles, kFlagThreads, s, b, L);
+  launch_pdl(tree_scan_kernel, L.nseg, kScanThreads, s, b, L, root_size, frames, c->st);
+  launch_pdl(tree_emit_kernel, L.flag_tiles, kFlagThreads, s, b, L, c->st);
   if (com_mode == kComJs)
-    tree_leaves_kernel<kComJs><<<L.flag_tiles, kLeafThreads, 0, s>>>(b, L, pos, stride, c->st);
+    launch_pdl(tree_leaves_kernel<kComJs>, L.flag_tiles, kLeafThreads, s, b, L, pos, stride, c->st);
   else if (com_mode == kComF64)
-    tree_leaves_kernel<kComF64><<<L.flag_tiles, kLeafThreads, 0, s>>>(b, L, pos, stride, c->st);
+    launch_pdl(tree_leaves_kernel<kComF64>, L.flag_tiles, kLeafThreads, s, b, L, pos, stride, c->st);
   else
-    tree_leaves_kernel<kComF32><<<L.flag_tiles, kLeafThreads, 0, s>>>(b, L, pos, stride, c->st);
+    launch_pdl(tree_leaves_kernel<kComF32>, L.flag_tiles, kLeafThreads, s, b, L, pos, stride, c->st);
 }
 
 void enqueue_walk(gs_ctx* c, int sf) {
@@ -525,7 +544,7 @@ void enqueue_walk(gs_ctx* c, int sf) {
   const int v = (sf ? 1 : 0) | (c->debug ? 2 : 0) | (one ? 4 : 0) | (c->walk_comp ? 8 : 0);
   switch (v) {
 #define GS_WALK_CASE(V, SF, DBG, ONE, COMP) \
-  case V: walk_kernel<SF, DBG, ONE, COMP><<<g, kWalkThreads, 0, s>>>(a); break;
+  case V: launch_pdl(walk_kernel<SF, DBG, ONE, COMP>, g, kWalkThreads, s, a); break;
     GS_WALK_CASE(0, false, false, false, false)
     GS_WALK_CASE(1, true, false, false, false)
     GS_WALK_CASE(2, false, true, false, false)
@@ -545,8 +564,8 @@ void enqueue_walk(gs_ctx* c, int sf) {
 #undef GS_WALK_CASE
   }
   // per-galaxy FP64 diagnostics of this walk
-  diag_reduce_kernel<<<c->lay.diag_chunks, dim3(32, kPartials), 0, s>>>(c->partials, c->lay, c->diag_chunk,
-                                                                         c->diag_ctr, c->diag_out);
+  launch_pdl(diag_reduce_kernel, c->lay.diag_chunks, dim3(32, kPartials), s, (const double*)c->partials, c->lay,
+             c->diag_chunk, c->diag_ctr, c->diag_out);
   c->cur ^= 1;
 }
 
@@ -556,11 +575,14 @@ void enqueue_sort_build(gs_ctx* c, int advance_time) {
   const Layout& L = c->lay;
   enqueue_codes_sort(c, c->part[c->cur], 2, advance_time);
   enqueue_sort_passes(c, track);
-  gather_kernel<<<L.flag_tiles, kTileThreads, 0, c->stream>>>(
-      c->vals[0], c->part[c->cur], c->part[c->cur ^ 1], c->stel[c->scur], c->stel[c->scur ^ 1], L, c->st);
+  launch_pdl(gather_kernel, L.flag_tiles, kTileThreads, c->stream, (const uint32_t*)c->vals[0],
+             (const float4*)c->part[c->cur], c->part[c->cur ^ 1], (const float4*)c->stel[c->scur],
+             c->stel[c->scur ^ 1], L, c->st);
   c->cur ^= 1;
   c->scur ^= 1;
-  if (track) track_kernel<<<cdiv(L.nseg, 128), 128, 0, c->stream>>>(c->inv, c->part[c->cur], L, c->st);
+  if (track)
+    launch_pdl(track_kernel, cdiv(L.nseg, 128), 128, c->stream, (const uint32_t*)c->inv,
+               (const float4*)c->part[c->cur], L, c->st);
   enqueue_build(c, c->part[c->cur], 2, c->com_mode, 0.0, c->frames);
 }
 
@@ -1558,7 +1580,7 @@ int gs_morton_codes(const float* pos, uint32_t N, uint32_t stride, uint32_t* cod
   TK(cudaMemcpyAsync(c->part[0], h.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, c->stream), "upload");
   const Layout& L = c->lay;
   bbox_kernel<<<L.flag_tiles, kTileThreads, 0, c->stream>>>(c->part[0], 1, L, c->bbox_part, c->seg_ctr,
-                                                            c->frames, c->st, 0);
+                                                            c->frames, c->st, 0, nullptr, 0u, nullptr, 0u);
   codes_kernel<<<L.flag_tiles, kTileThreads, 0, c->stream>>>(c->part[0], 1, L, c->frames, c->keys[0], nullptr,
                                                              0);
   TK(cudaGetLastError(), "codes");

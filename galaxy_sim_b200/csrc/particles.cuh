@@ -43,9 +43,17 @@ __device__ inline TileRange tile_range(const Layout& L, uint32_t tile) {
 // last tile folds its partials, derives the double frame (:53-54) and, with
 // advance_time, stamps Params.time = f32(simTime) and advances simTime by dt
 // (main.js:422, :476). seg_ctr[slot] counts finished tiles and self-resets.
+// It also clears the sort's scratch for this step (zero0[n0], zero1[n1]: digit
+// histograms, tile counters, look-back words), which the next kernels fill.
 __global__ void __launch_bounds__(kTileThreads)
     bbox_kernel(const float4* __restrict__ pos, uint32_t stride, Layout L, int* partials,
-                unsigned* seg_ctr, MortonFrame* frames, DevState* st, int advance_time) {
+                unsigned* seg_ctr, MortonFrame* frames, DevState* st, int advance_time,
+                uint32_t* zero0, uint32_t n0, uint32_t* zero1, uint32_t n1) {
+  griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n0 + n1; k += gridDim.x * blockDim.x) {
+    if (k < n0) zero0[k] = 0u;
+    else zero1[k - n0] = 0u;
+  }
   __shared__ int s_red[kTileThreads / 32][6];
   __shared__ bool s_last;
   const TileRange t = tile_range(L, blockIdx.x);
@@ -144,6 +152,7 @@ __global__ void __launch_bounds__(kTileThreads)
     codes_kernel(const float4* __restrict__ pos, uint32_t stride, Layout L,
                  const MortonFrame* __restrict__ frames, uint32_t* __restrict__ codes,
                  uint32_t* hist, int passes) {
+  griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
   __shared__ uint32_t s_hist[kSortPasses * 256];
   const TileRange t = tile_range(L, blockIdx.x);
   if (hist)
@@ -196,6 +205,7 @@ __global__ void __launch_bounds__(kTileThreads)
     gather_kernel(const uint32_t* __restrict__ perm, const float4* __restrict__ pin,
                   float4* __restrict__ pout, const float4* __restrict__ sin,
                   float4* __restrict__ sout, Layout L, DevState* st) {
+  griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
   const TileRange t = tile_range(L, blockIdx.x);
 #pragma unroll
   for (int q = 0; q < kTilePer; q++) {
@@ -219,6 +229,7 @@ __global__ void __launch_bounds__(kTileThreads)
 // double like the JS numbers); its f32 copy goes to Params (NBodyGPU.js:272-273).
 __global__ void track_kernel(const uint32_t* __restrict__ inv, const float4* __restrict__ P,
                              Layout L, DevState* st) {
+  griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= L.nseg) return;
   const SegDesc sd = L.segs[r];
@@ -361,6 +372,7 @@ constexpr uint32_t kDiagChunk = 512;
 __global__ void __launch_bounds__(32 * kPartials)
     diag_reduce_kernel(const double* __restrict__ partials, Layout L, double* chunk_part,
                        unsigned* diag_ctr, double* out) {
+  griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
   __shared__ bool s_last;
   const uint32_t x = blockIdx.x;
   uint32_t lo = 0, hi = L.nseg;

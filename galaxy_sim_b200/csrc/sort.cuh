@@ -55,6 +55,7 @@ __global__ void __launch_bounds__(kSortThreads)
                   uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
                   uint32_t* __restrict__ inv_out, const uint32_t* __restrict__ hist, int pass,
                   uint32_t* lookback, uint32_t* tile_counter, Layout L, DevState* st) {
+  griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kSortWarps][256];
   __shared__ uint32_t s_prefix[256];

@@ -205,6 +205,7 @@ __device__ inline void prefetch_l1(const void* p) {
 // plainly into the same sums.
 template <bool SF, bool DBG, bool ONE, bool COMP>
 __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(WalkArgs a) {
+  griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
   __shared__ WalkSmem smem_all[kWalkWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   WalkSmem& S = smem_all[warp];
