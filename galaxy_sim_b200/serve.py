@@ -102,6 +102,7 @@ def summarize(requests, step_ms, wall_s) -> dict:
     lat = [r.finished - r.arrival for r in requests]
     wait = [r.admitted - r.arrival for r in requests]
     return {"particle_steps": int(ps), "wall_s": round(wall_s, 3),
+            "gpu_busy_s": round(sum(step_ms) / 1e3, 3),
             "value": round(ps / wall_s, 1) if wall_s > 0 else None,
             "step_ms": {"p50": _pct(step_ms, 0.5), "p99": _pct(step_ms, 0.99), "n": len(step_ms)},
             "request_s": {"p50": _pct(lat, 0.5), "p99": _pct(lat, 0.99)},
