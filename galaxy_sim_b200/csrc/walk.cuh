@@ -36,6 +36,7 @@ constexpr int kPartials = 6;  // e_diag, e_true, px, py, pz, mass
 #define GS_WALK_RANGES 4
 #endif
 constexpr int kWalkRanges = GS_WALK_RANGES;  // child ranges popped and tested per round (1..4)
+static_assert(kWalkRanges >= 1 && kWalkRanges <= 4, "a round stages at most one child per lane");
 // ranges; a round explores kWalkRanges paths, each leaving <= 7 pending ranges per depth
 constexpr int kWalkStack = 8 * 11 * kWalkRanges;
 #ifndef GS_WALK_BLOCKS_PER_SM
@@ -123,7 +124,7 @@ struct WalkSmem {
   uint32_t cnode[8 * kWalkRanges];  // node index of each staged child
   uint4 cmeta[8 * kWalkRanges];     // {child, info, own-leaf density bits, massive}
   float lx[66], ly[66], lz[66], lm[66];
-  uint4 bl[4];                      // leaf batch: {first particle, count, lane mask, 0}
+  uint4 bl[8 * kWalkRanges];        // opened small leaves: {first particle, count, lane mask, 0}
 };
 
 // Direct sum of a staged leaf segment [off, off + k) for the lanes in `me`
@@ -195,8 +196,17 @@ __device__ inline float set_gt(float a, float b) {
   return r;
 }
 
-__device__ inline void prefetch_l1(const void* p) {
-  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+// Transpose of the 32 x 32 bit matrix held one row per lane: afterwards bit j
+// of lane i is bit i of lane j (five butterfly stages of 16, 8, 4, 2, 1 bits).
+__device__ __forceinline__ uint32_t warp_transpose(uint32_t x, int lane) {
+  const uint32_t m16 = 0x0000FFFFu, m8 = 0x00FF00FFu, m4 = 0x0F0F0F0Fu, m2 = 0x33333333u, m1 = 0x55555555u;
+#pragma unroll
+  for (int j = 16; j >= 1; j >>= 1) {
+    const uint32_t m = j == 16 ? m16 : j == 8 ? m8 : j == 4 ? m4 : j == 2 ? m2 : m1;
+    const uint32_t y = __shfl_xor_sync(0xffffffffu, x, j);
+    x = (lane & j) ? ((x & ~m) | ((y >> j) & m)) : ((x & m) | ((y & m) << j));
+  }
+  return x;
 }
 
 // ONE: the layout holds a single galaxy, whose descriptor comes with the
@@ -361,78 +371,83 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
         if (((actbits >> (cc >> 3)) & 1u) && (i - mt.x) < (mt.y & ~kLeafBit)) dens = __uint_as_float(mt.z);
       }
       if (!om) continue;
-      // opened internal children: push their child ranges
-      for (uint32_t bb = om & ~leafmask; bb; bb &= bb - 1) {
-        const uint32_t cc = __ffs(bb) - 1;
-        const unsigned open = __ballot_sync(full, (obits >> cc) & 1u);
-        const uint4 mt = S.cmeta[cc];
-        const uint32_t cchild = mt.x, ccnt = mt.y & ~kLeafBit;
-        // a galaxy's child ranges stay in its node range by construction (build,
-        // upload check); the walk itself only guards the pool bounds
-        if (!(cchild > S.cnode[cc] && (uint64_t)cchild + ccnt <= a.node_pool && ccnt >= 1u && ccnt <= 8u)) {
-          if (lane == 0) raise_err(sst, GS_DERR_TREE);
-          continue;
+      // Every slot's open mask at once: lane c's col holds the lanes that open
+      // slot c (the transpose of the 32 x 32 bit matrix whose rows are the lanes'
+      // obits), so each slot's lane can act on its own child in parallel.
+      const uint32_t col = warp_transpose(obits, lane);
+      // opened internal children: each slot's lane writes its child range and open
+      // mask to the stack, in slot order (prefix positions)
+      const uint32_t pushc = om & ~leafmask;
+      if (pushc) {
+        bool ok = false;
+        uint2 ent = make_uint2(0u, 0u);
+        if ((pushc >> lane) & 1u) {
+          const uint4 mt = S.cmeta[lane];
+          const uint32_t cchild = mt.x, ccnt = mt.y & ~kLeafBit;
+          // a galaxy's child ranges stay in its node range by construction (build,
+          // upload check); the walk itself only guards the pool bounds
+          ok = cchild > S.cnode[lane] && (uint64_t)cchild + ccnt <= a.node_pool && ccnt >= 1u && ccnt <= 8u;
+          if (!ok) raise_err(sst, GS_DERR_TREE);
+          ent = make_uint2(cchild | ((ccnt - 1u) << 29), col);
         }
-        if (sp >= kWalkStack) {  // cannot happen for depth <= 10 trees
-          if (lane == 0) raise_err(sst, GS_DERR_STACK);
-          continue;
-        }
-        if (lane == 0) S.stack[sp] = make_uint2(cchild | ((ccnt - 1u) << 29), open);
-        if (lane < (int)ccnt) {  // warm L1 for the range's staging load
-          prefetch_l1(&a.cm[cchild + lane]);
-          prefetch_l1(&a.info[cchild + lane]);
-        }
-        sp++;
+        const uint32_t okm = __ballot_sync(full, ok);
+        const int pos = sp + __popc(okm & ((1u << lane) - 1u));
+        if (ok && pos < kWalkStack) S.stack[pos] = ent;
+        const int np = __popc(okm);
+        if (sp + np > kWalkStack && lane == 0) raise_err(sst, GS_DERR_STACK);  // not for depth <= 10 trees
+        sp = min(sp + np, kWalkStack);
       }
-      // opened leaves: direct sums, two sources at a time; leaves of <= 16
-      // particles are staged four per batch (one load round), larger ones in chunks
-      uint32_t small = 0, big = 0;
-      for (uint32_t bb = om & leafmask; bb; bb &= bb - 1) {
-        const uint32_t cc = __ffs(bb) - 1;
-        const uint4 mt = S.cmeta[cc];
-        const uint32_t ccnt = mt.y & ~kLeafBit;
-        if ((uint64_t)mt.x + ccnt > a.pool_n) {
-          if (lane == 0) raise_err(sst, GS_DERR_TREE);
-          continue;
-        }
-        if (ccnt > 16u) big |= 1u << cc;
-        else small |= 1u << cc;
-      }
-      while (small) {
-        uint32_t nb = 0;
-        __syncwarp();
-        while (small && nb < 4) {
-          const uint32_t cc = __ffs(small) - 1;
-          small &= small - 1;
-          const unsigned open = __ballot_sync(full, (obits >> cc) & 1u);
-          const uint4 mt = S.cmeta[cc];
-          if (lane == 0) S.bl[nb] = make_uint4(mt.x, mt.y & ~kLeafBit, open, 0u);
-          nb++;
-        }
-        __syncwarp();
-#pragma unroll
-        for (int r = 0; r < 2; r++) {
-          const uint32_t e = lane + 32 * r, slot = e >> 4, q = e & 15u;
-          if (slot < nb) {
-            const uint4 bl = S.bl[slot];
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (q < bl.y) v = __ldg(&a.pin[2 * (size_t)(bl.x + q)]);
-            S.lx[e] = v.x;
-            S.ly[e] = v.y;
-            S.lz[e] = v.z;
-            S.lm[e] = v.w;
+      // opened leaves: direct sums, two sources at a time. Leaves of <= 16
+      // particles get their batch entries from their slots' lanes and are staged
+      // four per batch (one load round); larger ones go in chunks of 32.
+      const uint32_t leafc = om & leafmask;
+      uint32_t big = 0;
+      if (leafc) {
+        bool sm = false, bg = false;
+        uint4 ent = make_uint4(0u, 0u, 0u, 0u);
+        if ((leafc >> lane) & 1u) {
+          const uint4 mt = S.cmeta[lane];
+          const uint32_t ccnt = mt.y & ~kLeafBit;
+          if ((uint64_t)mt.x + ccnt > a.pool_n) {
+            raise_err(sst, GS_DERR_TREE);
+          } else {
+            bg = ccnt > 16u;
+            sm = !bg;
+            ent = make_uint4(mt.x, ccnt, col, 0u);
           }
         }
-        __syncwarp();
-        for (uint32_t sl = 0; sl < nb; sl++) {
-          const uint4 bl = S.bl[sl];
-          leaf_sum(S, 16 * sl, bl.y, i - bl.x, (bl.z >> lane) & 1u, soft, px, py, pz, eps2, ax, ay,
-                   az, pt, selfw, npair, DBG);
+        const uint32_t smallm = __ballot_sync(full, sm);
+        big = __ballot_sync(full, bg);
+        __syncwarp();  // earlier leaf sums are done reading the batch entries
+        if (sm) S.bl[__popc(smallm & ((1u << lane) - 1u))] = ent;
+        const uint32_t nsmall = __popc(smallm);
+        for (uint32_t b0 = 0; b0 < nsmall; b0 += 4) {
+          const uint32_t nb = min(4u, nsmall - b0);
+          __syncwarp();
+#pragma unroll
+          for (int r = 0; r < 2; r++) {
+            const uint32_t e = lane + 32 * r, slot = e >> 4, q = e & 15u;
+            if (slot < nb) {
+              const uint4 bl = S.bl[b0 + slot];
+              float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+              if (q < bl.y) v = __ldg(&a.pin[2 * (size_t)(bl.x + q)]);
+              S.lx[e] = v.x;
+              S.ly[e] = v.y;
+              S.lz[e] = v.z;
+              S.lm[e] = v.w;
+            }
+          }
+          __syncwarp();
+          for (uint32_t sl = 0; sl < nb; sl++) {
+            const uint4 bl = S.bl[b0 + sl];
+            leaf_sum(S, 16 * sl, bl.y, i - bl.x, (bl.z >> lane) & 1u, soft, px, py, pz, eps2, ax, ay,
+                     az, pt, selfw, npair, DBG);
+          }
         }
       }
       for (uint32_t bb = big; bb; bb &= bb - 1) {
         const uint32_t cc = __ffs(bb) - 1;
-        const unsigned open = __ballot_sync(full, (obits >> cc) & 1u);
+        const unsigned open = __shfl_sync(full, col, cc);
         const uint4 mt = S.cmeta[cc];
         const uint32_t cchild = mt.x, ccnt = mt.y & ~kLeafBit;
         for (uint32_t b0 = 0; b0 < ccnt; b0 += 32) {
