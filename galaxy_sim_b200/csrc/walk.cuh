@@ -327,12 +327,16 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
         const uint32_t cr = (cnts >> (4 * r)) & 15u;
         keep |= a_r ? ((1u << cr) - 1u) << (8 * r) : 0u;
       }
+      // theta^2 per range; a lane inactive for a range tests against -inf, so its
+      // td is -inf (or NaN) and it accepts and adds nothing there
+      float th2[kWalkRanges];
+#pragma unroll
+      for (int r = 0; r < kWalkRanges; r++) th2[r] = (actbits >> r) & 1u ? theta2 : -INFINITY;
       uint32_t obits = 0;  // children this lane opens (active, accept weight 0), bit = slot
 #pragma unroll
       for (int pp = 0; pp < 4 * kWalkRanges; pp++) {
         if (pp >= 4 * nr) break;
         const int c = 2 * pp;
-        const float2 actw = f2((actbits >> (pp >> 2)) & 1u ? 1.0f : 0.0f);
         const float2 qx = *reinterpret_cast<const float2*>(&S.cx[c]);
         const float2 qy = *reinterpret_cast<const float2*>(&S.cy[c]);
         const float2 qz = *reinterpret_cast<const float2*>(&S.cz[c]);
@@ -340,8 +344,8 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(Wa
         const float2 s2 = *reinterpret_cast<const float2*>(&S.cs2[c]);
         const float2 rx = __fadd2_rn(qx, px), ry = __fadd2_rn(qy, py), rz = __fadd2_rn(qz, pz);
         const float2 d2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __ffma2_rn(rz, rz, f2(eps2))));
-        const float2 td = __fmul2_rn(f2(theta2), d2);
-        const float2 w = __fmul2_rn(make_float2(set_gt(td.x, s2.x), set_gt(td.y, s2.y)), actw);
+        const float2 td = __fmul2_rn(f2(th2[pp >> 2]), d2);
+        const float2 w = make_float2(set_gt(td.x, s2.x), set_gt(td.y, s2.y));
         obits |= ((w.x == 0.0f ? 1u : 0u) | (w.y == 0.0f ? 2u : 0u)) << c;
         const float2 rinv = __fmul2_rn(make_float2(rsqrtf(d2.x), rsqrtf(d2.y)), w);
         const float2 mr = __fmul2_rn(qm, rinv);
