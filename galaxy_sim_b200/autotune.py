@@ -2,7 +2,7 @@
 
 The knobs never change results (`gs_set_tuning`): the persistent walk grid
 (blocks per SM; groups are independent, so fewer resident warps only change the
-schedule) and the sort tile (8 or 16 keys per thread; a stable sort has one
+schedule; below 8 the walk compiled for 72 registers per thread runs) and the sort tile (8 or 16 keys per thread; a stable sort has one
 answer). The bucket size (16) and the walk group (one warp of 32 particles)
 are not knobs: the first is the reference's tree, the second the warp.
 
@@ -16,9 +16,9 @@ from __future__ import annotations
 import ctypes as C
 import itertools
 
-from ._lib import TUNE_SORT_ITEMS, TUNE_WALK_BLOCKS_PER_SM, check, lib
+from ._lib import TUNE_SORT_ITEMS, TUNE_WALK_BLOCKS_PER_SM, GalaxyError, check, lib
 
-WALK_BLOCKS = (4, 6, 8)
+WALK_BLOCKS = (6, 7, 8)
 SORT_ITEMS = (8, 16)
 
 
@@ -42,8 +42,11 @@ def autotune(owner, steps: int = 5, warmup: int = 2, star_formation: bool = Fals
     ext = torch.cuda.ExternalStream(owner.stream, device=torch.device("cuda", device))
     timing = {}
     for bps, items in itertools.product(walk_blocks, sort_items):
-        set_(ctx, TUNE_WALK_BLOCKS_PER_SM, bps)
-        set_(ctx, TUNE_SORT_ITEMS, items)
+        try:
+            set_(ctx, TUNE_WALK_BLOCKS_PER_SM, bps)
+            set_(ctx, TUNE_SORT_ITEMS, items)
+        except GalaxyError:
+            continue  # beyond what this build's kernels were compiled for
         owner.run(warmup, star_formation)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(ext):

@@ -233,7 +233,7 @@ struct gs_ctx {
   bool single = false;  // created by gs_create: one galaxy, node pool 2N + 4096
   int com_mode = kComF32;
   int sort_items = kSortItems;     // tuning: keys per thread of a sort tile (8 or 16)
-  int walk_bps = kWalkBlocksPerSM; // tuning: persistent walk blocks per SM (1..8)
+  int walk_bps = kWalkBlocksPerSM; // tuning: persistent walk blocks per SM (1..8; < 8: 72-register build)
   bool walk_comp = false;  // Kahan-compensated far-field sums in the walk
   void* host_stage = nullptr;  // pinned: [slots] params
   std::map<int, cudaGraphExec_t> graphs;
@@ -520,6 +520,31 @@ void enqueue_build(gs_ctx* c, const float4* pos, uint32_t stride, int com_mode, 
     launch_pdl(tree_leaves_kernel<kComF32>, L.flag_tiles, kLeafThreads, s, b, L, pos, stride, c->st);
 }
 
+template <int MINB>
+void launch_walk(int v, uint32_t g, cudaStream_t s, const WalkArgs& a) {
+  switch (v) {
+#define GS_WALK_CASE(V, SF, DBG, ONE, COMP) \
+  case V: launch_pdl(walk_kernel<SF, DBG, ONE, COMP, MINB>, g, kWalkThreads, s, a); break;
+    GS_WALK_CASE(0, false, false, false, false)
+    GS_WALK_CASE(1, true, false, false, false)
+    GS_WALK_CASE(2, false, true, false, false)
+    GS_WALK_CASE(3, true, true, false, false)
+    GS_WALK_CASE(4, false, false, true, false)
+    GS_WALK_CASE(5, true, false, true, false)
+    GS_WALK_CASE(6, false, true, true, false)
+    GS_WALK_CASE(7, true, true, true, false)
+    GS_WALK_CASE(8, false, false, false, true)
+    GS_WALK_CASE(9, true, false, false, true)
+    GS_WALK_CASE(10, false, true, false, true)
+    GS_WALK_CASE(11, true, true, false, true)
+    GS_WALK_CASE(12, false, false, true, true)
+    GS_WALK_CASE(13, true, false, true, true)
+    GS_WALK_CASE(14, false, true, true, true)
+    GS_WALK_CASE(15, true, true, true, true)
+#undef GS_WALK_CASE
+  }
+}
+
 void enqueue_walk(gs_ctx* c, int sf) {
   WalkArgs a;
   a.pin = c->part[c->cur];
@@ -542,27 +567,9 @@ void enqueue_walk(gs_ctx* c, int sf) {
   if (one) a.seg0 = c->seg_host[0];
   else memset(&a.seg0, 0, sizeof(a.seg0));
   const int v = (sf ? 1 : 0) | (c->debug ? 2 : 0) | (one ? 4 : 0) | (c->walk_comp ? 8 : 0);
-  switch (v) {
-#define GS_WALK_CASE(V, SF, DBG, ONE, COMP) \
-  case V: launch_pdl(walk_kernel<SF, DBG, ONE, COMP>, g, kWalkThreads, s, a); break;
-    GS_WALK_CASE(0, false, false, false, false)
-    GS_WALK_CASE(1, true, false, false, false)
-    GS_WALK_CASE(2, false, true, false, false)
-    GS_WALK_CASE(3, true, true, false, false)
-    GS_WALK_CASE(4, false, false, true, false)
-    GS_WALK_CASE(5, true, false, true, false)
-    GS_WALK_CASE(6, false, true, true, false)
-    GS_WALK_CASE(7, true, true, true, false)
-    GS_WALK_CASE(8, false, false, false, true)
-    GS_WALK_CASE(9, true, false, false, true)
-    GS_WALK_CASE(10, false, true, false, true)
-    GS_WALK_CASE(11, true, true, false, true)
-    GS_WALK_CASE(12, false, false, true, true)
-    GS_WALK_CASE(13, true, false, true, true)
-    GS_WALK_CASE(14, false, true, true, true)
-    GS_WALK_CASE(15, true, true, true, true)
-#undef GS_WALK_CASE
-  }
+  // 8 blocks per SM: the 64-register build; fewer: the 72-register build
+  if (c->walk_bps >= kWalkBlocksPerSM) launch_walk<kWalkBlocksPerSM>(v, g, s, a);
+  else launch_walk<kWalkBlocksWide>(v, g, s, a);
   // per-galaxy FP64 diagnostics of this walk
   launch_pdl(diag_reduce_kernel, c->lay.diag_chunks, dim3(32, kPartials), s, (const double*)c->partials, c->lay,
              c->diag_chunk, c->diag_ctr, c->diag_out);
@@ -920,6 +927,7 @@ int gs_create_on(int device, uint32_t N, const float* particles8, const float* s
   }
   c->palloc.init(0);
   c->single = true;
+  c->walk_bps = kWalkBlocksWide;  // one galaxy: the 72-register walk measured faster
   return GS_OK;
 }
 

@@ -39,10 +39,10 @@ constexpr int kWalkRanges = GS_WALK_RANGES;  // child ranges popped and tested p
 static_assert(kWalkRanges >= 1 && kWalkRanges <= 4, "a round stages at most one child per lane");
 // ranges; a round explores kWalkRanges paths, each leaving <= 7 pending ranges per depth
 constexpr int kWalkStack = 8 * 11 * kWalkRanges;
-#ifndef GS_WALK_BLOCKS_PER_SM
-#define GS_WALK_BLOCKS_PER_SM 8
-#endif
-constexpr int kWalkBlocksPerSM = GS_WALK_BLOCKS_PER_SM;
+// The walk is compiled twice: for 8 resident blocks per SM (64 registers per
+// thread) and for 7 (72 registers, fewer spills); the launch tuning picks one.
+constexpr int kWalkBlocksPerSM = 8;
+constexpr int kWalkBlocksWide = 7;
 constexpr uint32_t kWalkGroup = 32;             // particles per warp (one per lane)
 
 // nbody_bh.wgsl:206-213
@@ -213,8 +213,9 @@ __device__ __forceinline__ uint32_t warp_transpose(uint32_t x, int lane) {
 // kernel parameters instead of a per-group lookup. COMP: far-field (monopole)
 // contributions are summed with Kahan compensation; near-field leaf sums add
 // plainly into the same sums.
-template <bool SF, bool DBG, bool ONE, bool COMP>
-__global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM) walk_kernel(WalkArgs a) {
+// MINB: resident blocks per SM the register budget is compiled for.
+template <bool SF, bool DBG, bool ONE, bool COMP, int MINB>
+__global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
   griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
   __shared__ WalkSmem smem_all[kWalkWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

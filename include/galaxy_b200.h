@@ -114,7 +114,9 @@ int gs_set_star_formation(gs_ctx* ctx, int enable);
  * this selects the precision variant; no counterpart in the reference. */
 int gs_set_walk_mode(gs_ctx* ctx, int compensated);
 /* Launch tuning that never changes results (no counterpart in the reference):
- * GS_TUNE_WALK_BLOCKS_PER_SM = persistent walk blocks per SM (1..8, default 8),
+ * GS_TUNE_WALK_BLOCKS_PER_SM = persistent walk blocks per SM (1..8; default 7 for a
+ * gs_create context, 8 for a pool; below 8 the walk built for 72 registers per
+ * thread runs),
  * GS_TUNE_SORT_ITEMS = keys per thread of a sort tile (8 or 16, default 16). Takes
  * effect at the next step; galaxy_sim_b200/autotune.py picks values by timing. */
 #define GS_TUNE_WALK_BLOCKS_PER_SM 1
