@@ -220,9 +220,11 @@ int gs_sort_and_build(const float* particles8, const float* stellar4, uint32_t N
  * gs_update_central_mass, gs_apply_permutation, gs_upload_tree, gs_read_positions,
  * gs_position_buffer, gs_stellar_buffer, gs_set_tracking, gs_get_tracking,
  * gs_get_tree, gs_read_state, gs_write_state, gs_read_forces, gs_energy,
- * gs_device_errors, gs_counters) act on the selected slot (gs_select, default 0)
- * and use that galaxy's own indices. gs_create makes a pool holding one galaxy in
- * slot 0. Each galaxy's results equal those of the same galaxy alone. */
+ * gs_device_errors, gs_counters, gs_set_star_formation) act on the selected slot
+ * (gs_select, default 0) and use that galaxy's own indices; gs_set_com_mode,
+ * gs_set_walk_mode, gs_set_debug and gs_set_tuning apply to the whole context.
+ * gs_create makes a pool holding one galaxy in slot 0. Each galaxy's results equal
+ * those of the same galaxy alone. */
 
 /* Free and total device memory of a CUDA device (cudaMemGetInfo). */
 int gs_device_memory(int device, uint64_t* free_bytes, uint64_t* total_bytes);
