@@ -122,7 +122,7 @@ struct WalkSmem {
   float cx[8 * kWalkRanges], cy[8 * kWalkRanges], cz[8 * kWalkRanges];  // staged child ranges
   float cmass[8 * kWalkRanges], cs2[8 * kWalkRanges];
   uint32_t cnode[8 * kWalkRanges];  // node index of each staged child
-  uint4 cmeta[8 * kWalkRanges];     // {child, info, own-leaf density bits, massive}
+  uint4 cmeta[8 * kWalkRanges];     // {child, info, own-leaf size bits, massive}
   float lx[66], ly[66], lz[66], lm[66];
   uint4 bl[8 * kWalkRanges];        // opened small leaves: {first particle, count, lane mask, 0}
 };
@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
         S.cs2[lane] = s2;
         S.cnode[lane] = rs + c;
         S.cmeta[lane] = make_uint4(w.child, w.info,
-                                   own ? __float_as_uint((float)wc / (w.size * w.size * w.size)) : 0u,
+                                   own ? __float_as_uint(w.size) : 0u,
                                    massive ? 1u : 0u);
       }
       const unsigned ownmask = __ballot_sync(full, own);  // leaves holding our particles
@@ -373,7 +373,11 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
       for (uint32_t bb = ownmask; bb; bb &= bb - 1) {  // own-leaf density (nbody_bh.wgsl:93-95)
         const uint32_t cc = __ffs(bb) - 1;
         const uint4 mt = S.cmeta[cc];
-        if (((actbits >> (cc >> 3)) & 1u) && (i - mt.x) < (mt.y & ~kLeafBit)) dens = __uint_as_float(mt.z);
+        const uint32_t cnt = mt.y & ~kLeafBit;
+        if (((actbits >> (cc >> 3)) & 1u) && (i - mt.x) < cnt) {
+          const float sz = __uint_as_float(mt.z);
+          dens = (float)cnt / (sz * sz * sz);
+        }
       }
       if (!om) continue;
       // Every slot's open mask at once: lane c's col holds the lanes that open
