@@ -290,18 +290,6 @@ __global__ void __launch_bounds__(kFlagThreads) tree_emit_kernel(BuildBuffers b,
   }
 }
 
-// Children of internal node p (pool index) of a galaxy: [child_base[p], + count).
-__device__ inline uint32_t child_count(const BuildBuffers& b, const TreeMeta& m, uint32_t node_off,
-                                       uint32_t p) {
-  const int d = b.depth[p];
-  const uint32_t cb = b.child_base[p];
-  const uint32_t pl = p - node_off;
-  const uint32_t level_end = m.level_start[d] + m.level_count[d];
-  const uint32_t next = (pl + 1 < level_end) ? __ldcg(&b.child_base[p + 1])
-                                             : node_off + m.level_start[d + 1] + m.level_count[d + 1];
-  return next - cb;
-}
-
 // COM precision modes of the leaves-up pass.
 enum ComMode : int {
   kComF32 = 0,   // refresh_level arithmetic (nbody_bh.wgsl:289-313), FP32
@@ -313,11 +301,20 @@ enum ComMode : int {
 // tile); leaf COM, then carry each finished node to its parent; the last child
 // to finish sums the parent (children in slot order).
 constexpr int kLeafThreads = kFlagTile;
+constexpr int kComChunk = 8;  // leaf particles loaded per round trip
 template <int MODE>
 __global__ void __launch_bounds__(kLeafThreads)
     tree_leaves_kernel(BuildBuffers b, Layout Lo, const float4* __restrict__ pos,
                        uint32_t pos_stride, DevState* st) {
   griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
+  // the galaxy's level table (a block's tile lies in one galaxy), for child counts
+  __shared__ uint32_t lvl_start[kDepths + 1], lvl_count[kDepths + 1];
+  if (threadIdx.x <= kDepths) {
+    const TreeMeta& m0 = b.meta[Lo.segs[Lo.seg_of_flag_tile[blockIdx.x]].slot];
+    lvl_start[threadIdx.x] = m0.level_start[threadIdx.x];
+    lvl_count[threadIdx.x] = m0.level_count[threadIdx.x];
+  }
+  __syncthreads();
   do {  // `continue` leaves the block's single iteration
     const uint32_t tile = blockIdx.x;
     const SegDesc sd = Lo.segs[Lo.seg_of_flag_tile[tile]];
@@ -337,29 +334,46 @@ __global__ void __launch_bounds__(kLeafThreads)
       continue;
     }
     const int d = b.depth[n];
+    int32_t p = b.parent[n];
     const float size = __double2float_rn(ldexp(m.root_size, -d));
+    // particles in index order; each chunk's loads are issued together, so a
+    // leaf of <= 16 particles costs two memory round trips instead of one per particle
     float4 c;
     if (MODE == kComJs) {
       double mm = 0, cx = 0, cy = 0, cz = 0;
-      for (uint32_t j = lo; j < hi; j++) {
-        const float4 p = pos[(size_t)j * pos_stride];
-        const double pm = p.w;
-        mm = __dadd_rn(mm, pm);
-        cx = __dadd_rn(cx, __dmul_rn((double)p.x, pm));
-        cy = __dadd_rn(cy, __dmul_rn((double)p.y, pm));
-        cz = __dadd_rn(cz, __dmul_rn((double)p.z, pm));
+      for (uint32_t j0 = lo; j0 < hi; j0 += kComChunk) {
+        float4 q[kComChunk];
+#pragma unroll
+        for (int k = 0; k < kComChunk; k++)
+          q[k] = j0 + k < hi ? pos[(size_t)(j0 + k) * pos_stride] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < kComChunk; k++) {
+          if (j0 + k >= hi) break;
+          const double pm = q[k].w;
+          mm = __dadd_rn(mm, pm);
+          cx = __dadd_rn(cx, __dmul_rn((double)q[k].x, pm));
+          cy = __dadd_rn(cy, __dmul_rn((double)q[k].y, pm));
+          cz = __dadd_rn(cz, __dmul_rn((double)q[k].z, pm));
+        }
       }
       const double inv = mm > 0 ? __ddiv_rn(1.0, mm) : 0.0;
       c = make_float4(__double2float_rn(__dmul_rn(cx, inv)), __double2float_rn(__dmul_rn(cy, inv)),
                       __double2float_rn(__dmul_rn(cz, inv)), __double2float_rn(mm));
     } else {
       float mm = 0, cx = 0, cy = 0, cz = 0;
-      for (uint32_t j = lo; j < hi; j++) {
-        const float4 p = pos[(size_t)j * pos_stride];
-        cx = fmaf(p.x, p.w, cx);
-        cy = fmaf(p.y, p.w, cy);
-        cz = fmaf(p.z, p.w, cz);
-        mm += p.w;
+      for (uint32_t j0 = lo; j0 < hi; j0 += kComChunk) {
+        float4 q[kComChunk];
+#pragma unroll
+        for (int k = 0; k < kComChunk; k++)
+          q[k] = j0 + k < hi ? pos[(size_t)(j0 + k) * pos_stride] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < kComChunk; k++) {
+          if (j0 + k >= hi) break;
+          cx = fmaf(q[k].x, q[k].w, cx);
+          cy = fmaf(q[k].y, q[k].w, cy);
+          cz = fmaf(q[k].z, q[k].w, cz);
+          mm += q[k].w;
+        }
       }
       c = mm > 0.0f ? make_float4(cx / mm, cy / mm, cz / mm, mm) : make_float4(0.f, 0.f, 0.f, mm);
     }
@@ -371,43 +385,62 @@ __global__ void __launch_bounds__(kLeafThreads)
     w.size = size;
     b.info[n] = w;
     // carry upwards
-    while (true) {
-      const int32_t p = b.parent[n];
-      if (p < 0) break;
-      const uint32_t nc =
-          ((uint32_t)p < n && (uint32_t)p >= sd.node_off) ? child_count(b, m, sd.node_off, (uint32_t)p) : 0u;
-      if ((uint32_t)p >= n || (uint32_t)p < sd.node_off || nc == 0 || nc > 8 ||
-          (uint64_t)b.child_base[p] + nc > node_end) {  // parents precede children in BFS
+    while (p >= 0) {
+      const uint32_t up = (uint32_t)p;
+      if (up >= n || up < sd.node_off) {  // parents precede children in BFS
+        raise_err(st + sd.slot, GS_DERR_NODES);
+        break;
+      }
+      // the parent's structure (read-only here), loads issued together; its child
+      // range ends where the next node's begins, or at the end of the next level
+      const int dp = b.depth[up];
+      const uint32_t cb = b.child_base[up];
+      const uint32_t cb1 = b.child_base[up + 1];  // up + 1 <= n: inside the galaxy's nodes
+      const int32_t pp = b.parent[up];
+      if (dp < 0 || dp >= kMaxLevel) {  // internal nodes lie at depths 0..9
+        raise_err(st + sd.slot, GS_DERR_NODES);
+        break;
+      }
+      const uint32_t next = (up - sd.node_off + 1 < lvl_start[dp] + lvl_count[dp])
+                                ? cb1
+                                : sd.node_off + lvl_start[dp + 1] + lvl_count[dp + 1];
+      const uint32_t nc = next - cb;
+      if (nc == 0 || nc > 8 || (uint64_t)cb + nc > node_end) {
         raise_err(st + sd.slot, GS_DERR_NODES);
         break;
       }
       // release: this node's COM is visible before the count; acquire: the last
       // arriver sees every sibling's COM
-      const uint32_t old = cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(b.arrive[p])
+      const uint32_t old = cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(b.arrive[up])
                                .fetch_add(1u, cuda::memory_order_acq_rel);
       if (old + 1 != nc) break;
-      b.arrive[p] = 0;
-      const uint32_t cb = b.child_base[p];
+      b.arrive[up] = 0;
+      // the (at most 8) children's COMs, loads issued together, summed in slot order
+      float4 q[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) q[k] = k < (int)nc ? __ldcg(&b.cm[cb + k]) : make_float4(0.f, 0.f, 0.f, 0.f);
       float4 pc;
       if (MODE == kComF32) {
         float mm = 0, cx = 0, cy = 0, cz = 0;
-        for (uint32_t k = 0; k < nc; k++) {
-          const float4 q = __ldcg(&b.cm[cb + k]);
-          cx = fmaf(q.x, q.w, cx);
-          cy = fmaf(q.y, q.w, cy);
-          cz = fmaf(q.z, q.w, cz);
-          mm += q.w;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          if (k >= (int)nc) break;
+          cx = fmaf(q[k].x, q[k].w, cx);
+          cy = fmaf(q[k].y, q[k].w, cy);
+          cz = fmaf(q[k].z, q[k].w, cz);
+          mm += q[k].w;
         }
         pc = mm > 0.0f ? make_float4(cx / mm, cy / mm, cz / mm, mm) : make_float4(0.f, 0.f, 0.f, mm);
       } else {
         double mm = 0, cx = 0, cy = 0, cz = 0;
-        for (uint32_t k = 0; k < nc; k++) {
-          const float4 q = __ldcg(&b.cm[cb + k]);
-          const double qm = q.w;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          if (k >= (int)nc) break;
+          const double qm = q[k].w;
           mm = __dadd_rn(mm, qm);
-          cx = __dadd_rn(cx, __dmul_rn((double)q.x, qm));
-          cy = __dadd_rn(cy, __dmul_rn((double)q.y, qm));
-          cz = __dadd_rn(cz, __dmul_rn((double)q.z, qm));
+          cx = __dadd_rn(cx, __dmul_rn((double)q[k].x, qm));
+          cy = __dadd_rn(cy, __dmul_rn((double)q[k].y, qm));
+          cz = __dadd_rn(cz, __dmul_rn((double)q[k].z, qm));
         }
         if (MODE == kComJs) {
           const double inv = mm > 0 ? __ddiv_rn(1.0, mm) : 0.0;
@@ -420,16 +453,16 @@ __global__ void __launch_bounds__(kLeafThreads)
                       : make_float4(0.f, 0.f, 0.f, __double2float_rn(mm));
         }
       }
-      const int dp = b.depth[p];
       const float psize = __double2float_rn(ldexp(m.root_size, -dp));
-      b.cm[p] = pc;
+      b.cm[up] = pc;
       WalkInfo pw;
       pw.s2 = psize * psize;
       pw.child = cb;
       pw.info = nc;
       pw.size = psize;
-      b.info[p] = pw;
-      n = (uint32_t)p;
+      b.info[up] = pw;
+      n = up;
+      p = pp;
     }
   } while (0);
 }
