@@ -12,7 +12,7 @@ The oracle restates galaxy-sim's gravity path on the CPU:
   same tree, direct O(N^2) sum, analytic halo.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
-may import this package, as the checker or the timed CPU baseline; the product
+may import this package, as the test reference or the timed CPU baseline; the product
 package ``galaxy_sim_b200`` never does.
 
 Parity pinning: the reference's tests pin only the gather convention

@@ -8,7 +8,7 @@
  *     kick-drift, star formation, permutation gather, position compaction)
  *
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load
- * this code, and only as the checker or the timed CPU baseline. The product
+ * this code, and only as the test reference or the timed CPU baseline. The product
  * path (galaxy_sim_b200) never calls it.
  *
  * Parity pinning: the reference's own tests pin only the gather direction

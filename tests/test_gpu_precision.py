@@ -13,8 +13,8 @@ acceptance rule on the same tree, against a direct FP64 O(N^2) sum over a seeded
 so this system's energy changes physically; the variants must agree on it.
 GPU FP64 is used only by the internal-node COM sums (com64) and the
 energy/momentum diagnostics.
-The figures are printed and, when a gpurun_out/ folder exists, written to
-gpurun_out/precision.json.
+The figures are printed and, when the environment variable GS_RESULTS_DIR names
+a folder, also written to $GS_RESULTS_DIR/precision.json.
 """
 import json
 import os
@@ -90,8 +90,8 @@ def test_precision_study(gpu_lib, oracle):
               f"{r['vs_fp64_walk']['p99']:.2e} | vs direct FP64 (32768) median "
               f"{r['vs_direct_fp64']['median']:.2e} p99 {r['vs_direct_fp64']['p99']:.2e} | "
               f"dE/E over {STEPS} steps {r['energy_drift']:+.3e}")
-    out = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "gpurun_out")
-    if os.path.isdir(out):
+    out = os.environ.get("GS_RESULTS_DIR", "")
+    if out and os.path.isdir(out):
         with open(os.path.join(out, "precision.json"), "w") as f:
             json.dump(rows, f, indent=1)
     # The halos follow the tracked black holes, a time-dependent external potential,
