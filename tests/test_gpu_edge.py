@@ -8,11 +8,15 @@
   depth-10 chains.
 Each must build the reference's tree, walk with forces inside the FP64-walk
 tolerance, raise no device error, and step identically alone and in a pool.
+* Uploaded trees that break the layout rules are flagged, never followed out of
+  bounds, and leave the context usable.
 """
 import numpy as np
 import pytest
 
+from galaxy_sim_b200 import _lib
 from galaxy_sim_b200 import initial_conditions as ic
+from galaxy_sim_b200 import morton_tree as mt
 from galaxy_sim_b200.nbody_gpu import NBodyGPU
 from galaxy_sim_b200.pool import GalaxyPool
 
@@ -77,3 +81,110 @@ def test_degenerate_inputs(gpu_lib, oracle, make):
     assert np.all(np.isfinite(got_P))
     assert pool.device_errors(s) == 0
     pool.close()
+
+
+def _corrupt(nodes, N, how):
+    """A copy of a valid BHNode array broken one way (the NBodyGPU upload rules:
+    children are a contiguous increasing run after their parent, leaves stay
+    inside the particle array)."""
+    bad = nodes.copy()
+    internal = [k for k in np.where(bad["isLeaf"] == 0)[0] if np.count_nonzero(bad["children"][k] >= 0) >= 2]
+    k = internal[len(internal) // 2]
+    ch = bad["children"][k]
+    first = int(ch[ch >= 0][0])
+    slots = np.where(ch >= 0)[0]
+    if how == "gap":          # second child skips a node
+        bad["children"][k, slots[1]] = first + 2
+    elif how == "range":      # a child past the node array
+        bad["children"][k, slots[0]] = len(nodes) + 5
+    elif how == "backward":   # a child that points back at its parent
+        bad["children"][k, slots[0]] = k
+    elif how == "leaf":       # a leaf running past the particle array
+        leaf = int(np.where(bad["isLeaf"] == 1)[0][-1])
+        bad["first"][leaf] = N - 1
+        bad["count"][leaf] = 16
+    return bad
+
+
+@pytest.mark.parametrize("how", ["gap", "range", "backward", "leaf"])
+def test_malformed_uploaded_tree_is_flagged(gpu_lib, how):
+    """uploadBHTree of a tree that breaks the layout rules raises GS_EDEVICE with
+    GS_DERR_TREE; the broken nodes become empty leaves, so a step over that tree
+    still ends, in bounds, with finite results; and the context stays usable: the
+    valid tree uploaded afterwards gives exactly what a fresh context gives."""
+    g = ic.disk_16k()
+    boot = mt.sortAndBuild(g.particles.ravel(), g.stellar.ravel(), g.N)
+    tree = boot["tree"]
+    nodes = tree.nodes[: tree.numNodes]
+    kw = dict(dt=0.005, G=1.0, epsilon=0.05, theta=0.5, haloMass=g.halo_mass, haloA=g.halo_a,
+              haloCenters=[[0, 0, 0, 0]])
+    fresh = NBodyGPU(0, boot["sorted"], boot["sortedStellar"])
+    fresh.uploadBHTree(nodes, tree.numNodes, tree.levelRanges)
+    fresh.updateParams(**kw)
+    fresh.encodeRefresh()
+    fresh.step()
+    want, _ = fresh.readState()
+    fresh.destroy()
+
+    sim = NBodyGPU(0, boot["sorted"], boot["sortedStellar"])
+    sim.updateParams(**kw)
+    with pytest.raises(_lib.GalaxyError) as e:
+        sim.uploadBHTree(_corrupt(nodes, g.N, how), tree.numNodes, tree.levelRanges)
+    assert e.value.code == _lib.GS_EDEVICE
+    assert sim.deviceErrors(clear=True) == _lib.DERR_TREE
+    sim.encodeRefresh()
+    sim.step()
+    P, _ = sim.readState()  # raises if the walk over the flagged tree set any error bit
+    assert np.all(np.isfinite(P))
+    assert sim.deviceErrors() == 0
+    # the same context, back on the valid tree from the same start
+    sim.writeState(boot["sorted"], boot["sortedStellar"])
+    sim.uploadBHTree(nodes, tree.numNodes, tree.levelRanges)
+    sim.encodeRefresh()
+    sim.step()
+    got, _ = sim.readState()
+    assert sim.deviceErrors() == 0
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    sim.destroy()
+
+
+def test_uploaded_dag_walk_is_bounded(gpu_lib):
+    """A tree that obeys the upload rules but shares children between parents
+    (node k's children are [k+1, k+2] down a chain of 40) has Fibonacci-many
+    root-to-leaf paths. The walk's round budget and stack bound end every group
+    with GS_DERR_STACK instead of running on; the context stays usable."""
+    g = ic.galaxy_disk(64, 41)
+    chain = 40
+    nodes = np.zeros(chain + 2, _lib.NODE_DTYPE)
+    nodes["mass"] = 1.0
+    nodes["size"] = 1.0e6          # opened by every particle
+    nodes["children"] = -1
+    for k in range(chain):
+        nodes["children"][k, 0], nodes["children"][k, 1] = k + 1, k + 2
+    for j, leaf in enumerate((chain, chain + 1)):
+        nodes["isLeaf"][leaf] = 1
+        nodes["first"][leaf], nodes["count"][leaf] = 32 * j, 32
+    kw = dict(dt=0.005, G=1.0, epsilon=0.05, theta=0.5)
+    sim = NBodyGPU(0, g.particles, g.stellar)
+    sim.updateParams(**kw)
+    sim.uploadBHTree(nodes, len(nodes))      # passes the layout rules
+    assert sim.deviceErrors() == 0
+    sim.step()
+    with pytest.raises(_lib.GalaxyError) as e:
+        sim.readState()
+    assert e.value.code == _lib.GS_EDEVICE
+    assert sim.deviceErrors(clear=True) & _lib.DERR_STACK
+    # the same context walks a proper tree afterwards, exactly like a fresh one
+    boot = mt.sortAndBuild(g.particles.ravel(), g.stellar.ravel(), g.N)
+    tree = boot["tree"]
+    outs = []
+    for ctx in (sim, NBodyGPU(0, boot["sorted"], boot["sortedStellar"])):
+        ctx.writeState(boot["sorted"], boot["sortedStellar"])
+        ctx.updateParams(**kw)
+        ctx.uploadBHTree(tree.nodes, tree.numNodes, tree.levelRanges)
+        ctx.encodeRefresh()
+        ctx.step()
+        outs.append(ctx.readState()[0])
+        assert ctx.deviceErrors() == 0
+        ctx.destroy()
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
