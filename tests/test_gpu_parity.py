@@ -189,6 +189,15 @@ def test_forces_disk512k(gpu_lib, oracle, big):
     _force_check(oracle, big, 0.02, 0.7, "disk512k theta 0.7")
 
 
+def test_forces_collision_and_sphere(gpu_lib, oracle):
+    """The other two presets: two disks 30 scale lengths apart (two far clusters
+    under one root, so the top levels are nearly empty) and a Hernquist sphere
+    (a cusp: deep leaves at the centre, sparse ones far out)."""
+    _force_check(oracle, ic.two_galaxy_collision(40000, 5), 0.02, 0.5, "collision 2x20000 theta 0.5")
+    _force_check(oracle, ic.hernquist_sphere(40000, 6), 0.02, 0.5, "sphere 40000 theta 0.5")
+    _force_check(oracle, ic.hernquist_sphere(40000, 6), 0.05, 0.7, "sphere 40000 theta 0.7")
+
+
 def test_reference_flow_upload_refresh_step(gpu_lib, oracle):
     """main.js init/loop on the NBodyGPU surface: sortAndBuild -> uploadBHTree ->
     updateParams -> encodeRefresh -> step -> readPositions, against the oracle."""
