@@ -1,0 +1,94 @@
+"""Calls beyond the NBodyGPU surface.
+
+* Checkpoint and restore: the particle and stellar records (gs_read_state /
+  gs_write_state), the simulation clock (gs_set_time) and the tracked centres
+  (gs_get_tracking / gs_set_tracking) are the whole state of a galaxy between
+  full steps, so a run stopped after 2 steps and resumed in a fresh context for 3
+  more equals an uninterrupted 5-step run bit for bit (star formation on, which
+  reads the clock; tracked halos on, which read the centres).
+* The walk's interaction counters (gs_counters) agree with the FP64 walk of the
+  same acceptance rule on the same tree, up to the few borderline acceptances
+  that FP32 and FP64 decide differently; reset returns and clears them.
+* gs_sync waits for queued work, bounded by a timeout.
+"""
+import numpy as np
+import pytest
+
+from galaxy_sim_b200 import initial_conditions as ic
+from galaxy_sim_b200.nbody_gpu import NBodyGPU
+from galaxy_sim_b200.simulation import Physics, Simulation, params_dict
+
+pytestmark = pytest.mark.gpu
+
+
+def _same(a, b):
+    return np.array_equal(np.asarray(a).view(np.uint32), np.asarray(b).view(np.uint32))
+
+
+def test_checkpoint_restore_continues_bit_identical(gpu_lib):
+    g = ic.two_galaxy_collision(20000, 7, gas_frac=0.3)
+    ph = Physics(0.02, 0.5, 0.005, gas_drag=0.25, sf_eff=0.05)
+    whole = Simulation(g, ph)
+    whole.run(5)
+    want_P, want_S = whole.gpu.readState()
+    want_tr = whole.gpu.getTracking()
+    want_e = whole.gpu.energy()
+    whole.close()
+
+    first = Simulation(g, ph)
+    first.run(2)
+    P2, S2 = first.gpu.readState()
+    c1, c2, h1, h2 = first.gpu.getTracking()
+    first.close()
+    t = 0.0  # the clock: a double advanced by the f32 dt once per full step
+    for _ in range(2):
+        t += float(np.float32(ph.dt))
+
+    resumed = NBodyGPU(0, P2, S2)
+    resumed.updateParams(**params_dict(g, ph))
+    resumed.setTime(t)
+    resumed.setTracking(c1, c2, h1, h2)
+    resumed.run(3, True)
+    got_P, got_S = resumed.readState()
+    got_tr = resumed.getTracking()
+    got_e = resumed.energy()
+    assert resumed.deviceErrors() == 0
+    resumed.destroy()
+    assert _same(got_P, want_P) and _same(got_S, want_S)
+    assert got_tr[:2] == want_tr[:2]
+    assert np.array_equal(got_tr[2], want_tr[2]) and np.array_equal(got_tr[3], want_tr[3])
+    assert got_e == want_e
+
+
+def test_walk_counters_match_the_fp64_walk(gpu_lib, oracle):
+    g = ic.disk_16k()
+    sim = NBodyGPU(0, g.particles, g.stellar)
+    sim.updateParams(dt=0.005, G=1.0, epsilon=0.05, theta=0.5)
+    sim.setDebug(True)
+    sim.sortBuild()
+    P, _ = sim.readState()
+    want = oracle.sort_and_build(g.particles, g.stellar)
+    com64 = oracle.refresh_f64(P, want["nodes"], want["levelRanges"])
+    sim.counters(reset=True)
+    sim.step()
+    mono, pairs, visits = sim.counters()
+    p = oracle.make_params(g.N, epsilon=0.05, theta=0.5, dt=0.005)
+    _, _, _, cnt = oracle.walk_f64(p, P, want["nodes"], com64)
+    assert mono > 0 and pairs > 0 and visits >= mono
+    assert abs(int(mono) - int(cnt[0])) <= 1e-3 * int(cnt[0]), (mono, cnt[0])
+    assert abs(int(pairs) - int(cnt[1])) <= 1e-3 * int(cnt[1]), (pairs, cnt[1])
+    assert sim.counters(reset=True) == [mono, pairs, visits]
+    assert sim.counters() == [0, 0, 0]
+    sim.destroy()
+
+
+def test_sync_waits_for_queued_steps(gpu_lib):
+    g = ic.disk_16k()
+    sim = NBodyGPU(0, g.particles, g.stellar)
+    sim.updateParams(dt=0.005, G=1.0, epsilon=0.05, theta=0.5)
+    assert sim.stream != 0
+    sim.run(20, False)
+    sim.sync(timeout_ns=10_000_000_000)  # returns once the 20 steps are done
+    P, _ = sim.readState()
+    assert np.all(np.isfinite(P)) and sim.deviceErrors() == 0
+    sim.destroy()
