@@ -136,3 +136,36 @@ def test_pool_accounting(gpu_lib):
     pool.remove(b)
     assert pool.free() == (10000, 2)
     pool.close()
+
+
+@pytest.mark.parametrize("comp,com64", [(True, False), (False, True), (True, True)],
+                         ids=["compensated", "com64", "both"])
+def test_batch_equals_solo_in_precision_modes(gpu_lib, comp, com64):
+    """The precision variants (Kahan-compensated far-field sums in the walk, FP64
+    internal-node COM) keep the batch guarantee: each galaxy equals its solo run
+    in the same mode, bit for bit."""
+    from galaxy_sim_b200 import _lib
+
+    cases = _cases()[:4]
+    steps = 2
+    solos = []
+    for g, ph in cases:
+        sim = NBodyGPU(0, g.particles, g.stellar)
+        sim.updateParams(**params_dict(g, ph))
+        t = _tracking(g)
+        if t is not None:
+            sim.setTracking(*t)
+        sim.setWalkMode(comp)
+        sim.setComMode(2 if com64 else 0)
+        sim.run(steps, True)
+        P, S = sim.readState()
+        solos.append((P, S, sim.energy(), sim.getTracking()))
+        sim.destroy()
+    pool = GalaxyPool(sum(g.N + 256 for g, _ in cases) + 4096, 8)
+    _lib.check(_lib.lib().gs_set_walk_mode(pool._ctx, int(comp)), pool._ctx)
+    _lib.check(_lib.lib().gs_set_com_mode(pool._ctx, 2 if com64 else 0), pool._ctx)
+    slots = [pool.add(g.particles, g.stellar, params_dict(g, ph), _tracking(g)) for g, ph in cases]
+    pool.run(steps, True)
+    for s, solo in zip(slots, solos):
+        _check_same(pool, s, solo)
+    pool.close()
