@@ -469,7 +469,7 @@ def walk_traffic(workload: str, theta: float):
     return int(round((float(m.group(1)) + float(m.group(2))) * 1e6)) if m else None
 
 
-def batch_compare(local, K, W):
+def batch_compare(local, K, W, tune=True):
     """Batched ensemble (one pool, one graph per step) vs the same galaxies as
     back-to-back plain runs, same GPU, same steps."""
     import torch
@@ -489,7 +489,7 @@ def batch_compare(local, K, W):
     pool.run(W, True)
     pool.sync()
     # launch knobs (walk grid, sort tile) picked by timing this batch; results do not depend on them
-    tuned = autotune(pool, steps=5, warmup=2, star_formation=True, device=local)
+    tuned = autotune(pool, steps=5, warmup=2, star_formation=True, device=local) if tune else None
     with Clocks(local) as clk:
         bms = _timed_steps(pool.stream, local, K, lambda: pool.run(1, True), flush)
     clocks = clk.summary()
@@ -565,7 +565,7 @@ def _mode_line(d):
 def run_batch(args, ws, rank, local):
     if rank != 0:
         return
-    print(json.dumps(_mode_line(batch_compare(local, args.steps, args.warmup))), flush=True)
+    print(json.dumps(_mode_line(batch_compare(local, args.steps, args.warmup, tune=not args.no_tune))), flush=True)
 
 
 def run_serve(args, ws, rank, local):
