@@ -189,6 +189,12 @@ def test_forces_disk512k(gpu_lib, oracle, big):
     _force_check(oracle, big, 0.02, 0.7, "disk512k theta 0.7")
 
 
+def test_forces_disk_largest_request(gpu_lib, oracle):
+    """The largest galaxy the served request mix holds (N = 2^20): device sort and
+    tree bit-exact, forces within the tolerance of the FP64 walk."""
+    _force_check(oracle, ic.disk_512k(seed=3, N=1 << 20), 0.02, 0.5, "disk 2^20 theta 0.5")
+
+
 def test_forces_collision_and_sphere(gpu_lib, oracle):
     """The other two presets: two disks 30 scale lengths apart (two far clusters
     under one root, so the top levels are nearly empty) and a Hernquist sphere
