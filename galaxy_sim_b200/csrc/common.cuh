@@ -10,7 +10,9 @@ namespace gs {
 constexpr int kBucket = 16;     // max particles per leaf (mortonTree.js:25)
 constexpr int kMaxLevel = 10;   // 10 bits per axis (mortonTree.js:26)
 constexpr int kDepths = 11;     // node depths 0..10
-constexpr uint32_t kSpinLimit = 1u << 24;  // iteration cap of every device-side wait
+// iteration cap of every device-side wait: about a second of polling (each
+// look-back iteration is one round trip of 32 loads to L2)
+constexpr uint32_t kSpinLimit = 1u << 20;
 
 // Walk-layout node (32 B, two 16-byte words), written by the build next to the
 // 64-byte BHNode layout of the API. Children of an internal node are the

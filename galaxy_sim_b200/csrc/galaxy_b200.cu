@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -472,7 +473,7 @@ void enqueue_codes_sort(gs_ctx* c, const float4* pos, uint32_t stride, int advan
 }
 
 template <int ITEMS>
-void sort_passes_items(gs_ctx* c, bool inv) {
+void sort_passes_items(gs_ctx* c, bool inv, uint32_t spin_limit, uint32_t withhold) {
   const Layout& L = c->lay;
   cudaStream_t s = c->stream;
   for (int p = 0; p < kSortPasses; p++) {
@@ -485,21 +486,23 @@ void sort_passes_items(gs_ctx* c, bool inv) {
     const uint32_t* h = c->hist();
     if (p == 0)
       launch_pdl(onesweep_pass<true, false, ITEMS>, L.sort_tiles, kSortThreads, s, kin, vin, c->keys[dst],
-                 c->vals[dst], iv, h, p, lb, ctr, L, c->st);
+                 c->vals[dst], iv, h, p, lb, ctr, L, c->st, spin_limit, withhold);
     else if (p < kSortPasses - 1)
       launch_pdl(onesweep_pass<false, false, ITEMS>, L.sort_tiles, kSortThreads, s, kin, vin, c->keys[dst],
-                 c->vals[dst], iv, h, p, lb, ctr, L, c->st);
+                 c->vals[dst], iv, h, p, lb, ctr, L, c->st, spin_limit, withhold);
     else
       launch_pdl(onesweep_pass<false, true, ITEMS>, L.sort_tiles, kSortThreads, s, kin, vin, c->keys[dst],
-                 c->vals[dst], iv, h, p, lb, ctr, L, c->st);
+                 c->vals[dst], iv, h, p, lb, ctr, L, c->st, spin_limit, withhold);
   }
 }
 
 // stable segmented sort of keys[0] -> keys[0] (sorted codes), vals[0] (gather
 // permutation) and, with inv, the inverse permutation; tile size per the tuning.
-void enqueue_sort_passes(gs_ctx* c, bool inv) {
-  if (c->sort_items == 8) sort_passes_items<8>(c, inv);
-  else sort_passes_items<16>(c, inv);
+// spin_limit / withhold: the look-back wait's failure-detection test settings
+// (production: kSpinLimit, no withheld tile).
+void enqueue_sort_passes(gs_ctx* c, bool inv, uint32_t spin_limit = kSpinLimit, uint32_t withhold = kNoTile) {
+  if (c->sort_items == 8) sort_passes_items<8>(c, inv, spin_limit, withhold);
+  else sort_passes_items<16>(c, inv, spin_limit, withhold);
 }
 
 // the trees over keys[0] (sorted codes) with COM from pos; root size from the
@@ -1557,6 +1560,10 @@ int tree_outputs(TmpCtx& t, uint32_t max_nodes, gs_node* nodes, uint32_t* num_no
   return GS_OK;
 }
 
+// Failure-detection settings of the two radix-sort entry points (gs_test_sort_lookback).
+std::atomic<uint32_t> g_test_spin_limit{kSpinLimit};
+std::atomic<uint32_t> g_test_withhold{kNoTile};
+
 __global__ void mask30_kernel(uint32_t* keys, uint32_t N) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
     keys[i] &= 0x3fffffffu;
@@ -1621,10 +1628,30 @@ int gs_radix_sort_indices(const uint32_t* codes, uint32_t N, uint32_t* perm) {
   mask30_kernel<<<grid_for(N, 256, 148 * 8), 256, 0, c->stream>>>(c->keys[0], N);
   TK(cudaMemsetAsync(c->sort_scratch, 0, sizeof(uint32_t) * c->plan.sort_words, c->stream), "clear");
   key_hist_kernel<<<L.flag_tiles, kTileThreads, 0, c->stream>>>(c->keys[0], L, c->hist(), kSortPasses);
-  enqueue_sort_passes(c, false);
+  enqueue_sort_passes(c, false, g_test_spin_limit.load(), g_test_withhold.load());
   TK(cudaGetLastError(), "sort");
   TK(cudaMemcpyAsync(perm, c->vals[0], sizeof(uint32_t) * N, cudaMemcpyDeviceToHost, c->stream), "perm");
   return tmp_check(t);
+}
+
+}  // extern "C"
+
+// The failure-detection settings, for the allocation-free sort in noalloc.cu.
+void gs_internal_sort_test_settings(uint32_t* spin_limit, uint32_t* withhold) {
+  *spin_limit = g_test_spin_limit.load();
+  *withhold = g_test_withhold.load();
+}
+
+extern "C" {
+
+int gs_test_sort_lookback(uint32_t spin_limit, int64_t withhold_tile) {
+  if (spin_limit == 0 || withhold_tile < -1 || withhold_tile >= (int64_t)kNoTile) {
+    set_err(g_err, "spin_limit must be positive and withhold_tile a tile index or -1");
+    return GS_EINVAL;
+  }
+  g_test_spin_limit.store(spin_limit);
+  g_test_withhold.store(withhold_tile < 0 ? kNoTile : (uint32_t)withhold_tile);
+  return GS_OK;
 }
 
 int gs_tree_build(const uint32_t* sorted_codes, const float* pos3, const float* masses, uint32_t N,

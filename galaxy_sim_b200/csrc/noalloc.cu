@@ -12,15 +12,26 @@
 //
 // The host code never hands the array's name to a kernel. In host code that
 // name only stands in for the device object, so a kernel given it would fault
-// or, where the GPU can reach host memory, silently use the wrong memory. The
-// first call on each device (with that device current) looks up the array's
-// device address with cudaGetSymbolAddress and caches it. That first call
-// should come before any stream capture.
+// or, where the GPU can reach host memory, silently use the wrong memory.
+// Set-up runs once per device context, with that device current: it looks up
+// the array's device address with cudaGetSymbolAddress and caches it, keyed by
+// the context's unique id so that a context reset (cudaDeviceReset) is noticed
+// and the address looked up again. Under lazy module loading the array and the
+// kernels' code are committed when first touched, so set-up also loads every
+// kernel of the sort and runs each once over no keys. A call with N == 0 does
+// only the set-up; callers make it at start-up, outside any stream capture, so
+// that later calls allocate nothing.
+//
+// Every call is synchronous (it reads the error word back and waits for the
+// stream), so it must never run inside a stream capture; a capturing stream is
+// rejected before anything is enqueued.
 //
 // All calls share the one array, and it keeps the contents of the last call.
 // Each call therefore clears the histograms, tile counters and look-back
-// words it relies on, and rewrites its one-galaxy layout, before using them. Calls whose work overlaps on the GPU
-// (two streams, or two host threads) race on that shared array: serialize them.
+// words it relies on, and rewrites its one-galaxy layout, before using them.
+// Calls whose work overlaps on the GPU (two streams, or two host threads) race
+// on that shared array: serialize them.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -31,6 +42,7 @@
 #include "sort.cuh"
 
 void gs_internal_set_error(const char* msg);
+void gs_internal_sort_test_settings(uint32_t* spin_limit, uint32_t* withhold);
 
 namespace {
 
@@ -55,8 +67,12 @@ static __device__ __align__(256) uint32_t g_noalloc_scratch[kScratchWords];  // 
 static __device__ DevState g_noalloc_state;                                   // error word
 
 constexpr int kMaxDevices = 64;
-void* g_scratch_addr[kMaxDevices];
-void* g_state_addr[kMaxDevices];
+struct DeviceSetup {
+  unsigned long long ctx_id = 0;  // the context the addresses belong to (0 = none yet)
+  void* scratch = nullptr;
+  void* state = nullptr;
+};
+DeviceSetup g_setup[kMaxDevices];
 std::mutex g_setup_mutex;
 
 // radixSortIndices orders by the low 30 bits (mortonTree.js:71-74): copy the
@@ -114,35 +130,92 @@ int cuda_fail(cudaError_t e, const char* what) {
   return e == cudaErrorMemoryAllocation ? GS_ENOMEM : GS_ECUDA;
 }
 
+// Unique id of the calling thread's current context (driver entry points,
+// resolved once through the runtime, so the library needs no libcuda link).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+
+int current_context_id(unsigned long long* id) {
+  if (!g_ctx_get_current || !g_ctx_get_id) {
+    void* f0 = nullptr;
+    void* f1 = nullptr;
+    cudaDriverEntryPointQueryResult q0, q1;
+    cudaError_t e = cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f0, 12000, cudaEnableDefault, &q0);
+    if (e == cudaSuccess)
+      e = cudaGetDriverEntryPointByVersion("cuCtxGetId", &f1, 12000, cudaEnableDefault, &q1);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDriverEntryPointByVersion");
+    if (q0 != cudaDriverEntryPointSuccess || q1 != cudaDriverEntryPointSuccess || !f0 || !f1)
+      return fail(GS_ECUDA, "the driver lacks cuCtxGetCurrent/cuCtxGetId");
+    g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f0);
+    g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f1);
+  }
+  CUcontext ctx = nullptr;
+  if (g_ctx_get_current(&ctx) != CUDA_SUCCESS) return fail(GS_ECUDA, "cuCtxGetCurrent failed");
+  *id = 0;
+  if (ctx && g_ctx_get_id(ctx, id) != CUDA_SUCCESS) return fail(GS_ECUDA, "cuCtxGetId failed");
+  return GS_OK;
+}
+
+// Set-up on the current device: load the module's array and kernels and look up
+// the array's device address, once per context. Returns the cached addresses.
+int setup_device(int dev, uint32_t** base, DevState** st) {
+  std::lock_guard<std::mutex> lock(g_setup_mutex);
+  DeviceSetup& d = g_setup[dev];
+  unsigned long long id = 0;
+  int rc = current_context_id(&id);
+  if (rc) return rc;
+  if (id == 0 || id != d.ctx_id) {
+    void* p = nullptr;
+    void* q = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(scratch)");
+    e = cudaGetSymbolAddress(&q, g_noalloc_state);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(state)");
+    // load the code of every kernel the sort launches (lazy loading would
+    // otherwise commit it on the first launch)
+    cudaFuncAttributes fa;
+    const void* kernels[] = {
+        reinterpret_cast<const void*>(noalloc_layout_kernel),
+        reinterpret_cast<const void*>(noalloc_mask_hist_kernel),
+        reinterpret_cast<const void*>(onesweep_pass<true, false>),
+        reinterpret_cast<const void*>(onesweep_pass<false, false>),
+    };
+    for (const void* k : kernels)
+      if ((e = cudaFuncGetAttributes(&fa, k)) != cudaSuccess) return cuda_fail(e, "cudaFuncGetAttributes");
+    if ((rc = current_context_id(&id))) return rc;  // the look-up made the context current
+    d.scratch = p;
+    d.state = q;
+    d.ctx_id = id;
+  }
+  *base = static_cast<uint32_t*>(d.scratch);
+  *st = static_cast<DevState*>(d.state);
+  return GS_OK;
+}
+
 }  // namespace
 
 extern "C" int gs_radix_sort_indices_noalloc(const uint32_t* d_codes, uint32_t N, uint32_t* d_perm,
                                              void* stream) {
-  if (N == 0) return GS_OK;
-  if (!d_codes || !d_perm) return fail(GS_EINVAL, "d_codes and d_perm must be device pointers");
   if (N > kNoAllocMaxN)
     return fail(GS_EINVAL, "gs_radix_sort_indices_noalloc: N exceeds its static scratch "
                            "(at most 1048576 codes)");
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-  if (dev < 0 || dev >= kMaxDevices) return fail(GS_EINVAL, "device ordinal out of range");
-  {
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[dev]) {  // once per device, with that device current
-      void* p = nullptr;
-      void* q = nullptr;
-      e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(scratch)");
-      e = cudaGetSymbolAddress(&q, g_noalloc_state);
-      if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(state)");
-      g_state_addr[dev] = q;
-      g_scratch_addr[dev] = p;
-    }
-  }
-  uint32_t* base = static_cast<uint32_t*>(g_scratch_addr[dev]);
-  DevState* st = static_cast<DevState*>(g_state_addr[dev]);
+  if (N && (!d_codes || !d_perm)) return fail(GS_EINVAL, "d_codes and d_perm must be device pointers");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(s, &cap);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamIsCapturing");
+  if (cap != cudaStreamCaptureStatusNone)
+    return fail(GS_EINVAL, "gs_radix_sort_indices_noalloc is synchronous and cannot run while its "
+                           "stream is capturing");
+  int dev = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices) return fail(GS_EINVAL, "device ordinal out of range");
+  uint32_t* base = nullptr;
+  DevState* st = nullptr;
+  int rc = setup_device(dev, &base, &st);
+  if (rc) return rc;
   uint32_t* k0 = base;
   uint32_t* k1 = base + kKeyWords;
   uint32_t* v0 = base + 2 * kKeyWords;
@@ -151,6 +224,25 @@ extern "C" int gs_radix_sort_indices_noalloc(const uint32_t* d_codes, uint32_t N
   uint32_t* lb = base + kLbOff;
   SegDesc* seg = reinterpret_cast<SegDesc*>(base + kSegOff);
   uint32_t* map = base + kMapOff;
+  if (N == 0) {
+    // the set-up call: every kernel of the sort runs once over no keys, so that
+    // its code and local memory are in place before the first real call
+    Layout E = {};
+    E.segs = seg;
+    E.seg_of_sort_tile = map;
+    E.nseg = 1;
+    noalloc_layout_kernel<<<1, 256, 0, s>>>(seg, map, 0, 0);
+    noalloc_mask_hist_kernel<<<1, 256, 0, s>>>(nullptr, 0, k0, hist);
+    onesweep_pass<true, false><<<1, kSortThreads, 0, s>>>(nullptr, nullptr, nullptr, nullptr, nullptr, hist, 0,
+                                                          lb, ctr, E, st);
+    onesweep_pass<false, false><<<1, kSortThreads, 0, s>>>(nullptr, nullptr, nullptr, nullptr, nullptr, hist, 1,
+                                                           lb, ctr + 1, E, st);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "set-up launch");
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    return GS_OK;
+  }
+  uint32_t spin_limit = kSpinLimit, withhold = kNoTile;
+  gs_internal_sort_test_settings(&spin_limit, &withhold);
   const uint32_t tiles = (N + kSortTile - 1) / kSortTile;
   // what must start at zero: histograms, tile counters, look-back words, error word
   if ((e = cudaMemsetAsync(hist, 0, kClearBytes, s)) != cudaSuccess) return cuda_fail(e, "clear");
@@ -178,10 +270,12 @@ extern "C" int gs_radix_sort_indices_noalloc(const uint32_t* d_codes, uint32_t N
     uint32_t* plb = lb + (size_t)p * kNoAllocTiles * 256;
     if (p == 0)
       onesweep_pass<true, false><<<tiles, kSortThreads, 0, s>>>(kin[p], nullptr, kout[p], vout[p], nullptr,
-                                                                hist, p, plb, ctr + p, L, st);
+                                                                hist, p, plb, ctr + p, L, st, spin_limit,
+                                                                withhold);
     else
       onesweep_pass<false, false><<<tiles, kSortThreads, 0, s>>>(kin[p], vin[p], kout[p], vout[p], nullptr,
-                                                                 hist, p, plb, ctr + p, L, st);
+                                                                 hist, p, plb, ctr + p, L, st, spin_limit,
+                                                                 withhold);
   }
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "sort launch");
   unsigned err = 0;

@@ -49,12 +49,18 @@ __device__ inline void hist_add_warp(uint32_t* s_hist, uint32_t key, bool valid,
 // inv_out is given (central-particle tracking).
 // hist: [slots][kSortPasses][256] digit counts of each galaxy; lookback: [sort tiles][256];
 // st: per-slot states (error word).
+// spin_limit: look-back iterations without progress before the tile gives up
+// (kSpinLimit in production). withhold: a tile that never publishes its digit
+// counts (kNoTile in production); the failure-detection tests set it so that
+// the successors' waits run out and raise GS_DERR_LOOKBACK.
+constexpr uint32_t kNoTile = 0xffffffffu;
 template <bool FIRST, bool LAST, int ITEMS = kSortItems>
 __global__ void __launch_bounds__(kSortThreads)
     onesweep_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                   uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
                   uint32_t* __restrict__ inv_out, const uint32_t* __restrict__ hist, int pass,
-                  uint32_t* lookback, uint32_t* tile_counter, Layout L, DevState* st) {
+                  uint32_t* lookback, uint32_t* tile_counter, Layout L, DevState* st,
+                  uint32_t spin_limit = kSpinLimit, uint32_t withhold = kNoTile) {
   griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kSortWarps][256];
@@ -125,12 +131,13 @@ __global__ void __launch_bounds__(kSortThreads)
   const uint32_t gexcl = sd.off + wpre + incl - h;
 
   uint32_t* lb = lookback + (size_t)tile * 256;
+  const bool publish = tile != withhold;
   uint32_t excl;
   if (lt == 0) {
     excl = gexcl;
-    st_relaxed(&lb[d], kLbInc | (gexcl + tot));
+    if (publish) st_relaxed(&lb[d], kLbInc | (gexcl + tot));
   } else {
-    st_relaxed(&lb[d], kLbAgg | tot);
+    if (publish) st_relaxed(&lb[d], kLbAgg | tot);
     excl = 0;
     int64_t t = (int64_t)lt - 1;  // predecessors within the galaxy
     uint32_t spins = 0;
@@ -157,12 +164,12 @@ __global__ void __launch_bounds__(kSortThreads)
         }
       }
       t -= used;
-      if (!done && used == 0 && ++spins > kSpinLimit) {
+      if (!done && used == 0 && ++spins > spin_limit) {
         raise_err(sst, GS_DERR_LOOKBACK);
         break;
       }
     }
-    st_relaxed(&lb[d], kLbInc | ((excl + tot) & kLbMask));
+    if (publish) st_relaxed(&lb[d], kLbInc | ((excl + tot) & kLbMask));
   }
   s_prefix[d] = excl;
   __syncthreads();

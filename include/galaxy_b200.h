@@ -197,6 +197,17 @@ int gs_morton_codes(const float* pos, uint32_t N, uint32_t stride, uint32_t* cod
                     double* root_size);
 /* radixSortIndices (mortonTree.js:68-84): stable sort -> gather permutation. */
 int gs_radix_sort_indices(const uint32_t* codes, uint32_t N, uint32_t* perm);
+/* Failure-detection test setting of gs_radix_sort_indices (and of
+ * gs_radix_sort_indices_noalloc), no counterpart in the reference. Every later
+ * call of those two sorts runs its digit passes with a look-back wait of at
+ * most spin_limit polls without progress (production: about a second) and,
+ * when withhold_tile >= 0, with that sort tile never publishing its digit
+ * counts, so the waits of the tiles after it run out: the call then returns
+ * GS_EDEVICE (GS_DERR_LOOKBACK) instead of hanging, its permutation is
+ * garbage, and every write stays inside the call's own buffers. The pools'
+ * step graphs never use this setting. gs_test_sort_lookback(1u << 20, -1)
+ * restores the production setting. */
+int gs_test_sort_lookback(uint32_t spin_limit, int64_t withhold_tile);
 /* MortonTree.build (mortonTree.js:107-182) over sorted codes, stride-3 positions
  * and masses; max_nodes follows the MortonTree pool (2N + 4096 there). */
 int gs_tree_build(const uint32_t* sorted_codes, const float* pos3, const float* masses,
@@ -260,10 +271,20 @@ int gs_pool_energies(gs_ctx* ctx, gs_diag* out, uint32_t cap);
  * the default stream). The call allocates nothing: its scratch is one static
  * device array for at most 1048576 codes (about 13 MiB), held by every GPU that
  * loads the library until the process exits; larger N is rejected with
- * GS_EINVAL. The first call on a device looks up that array's device address and
- * should come before any stream capture. Calls share the array, so calls whose
- * work overlaps on the GPU race: serialize them. Returns after the stream has
- * finished the sort. */
+ * GS_EINVAL.
+ * Set-up: under CUDA's default lazy module loading the array, and the code of
+ * the sort's kernels, are committed on the device the first time the library
+ * touches them. The first call on a device (and the first after the device's
+ * context was reset) therefore does that set-up: it loads the array's module
+ * and kernels and looks up the array's device address. A call with N == 0
+ * does only this set-up and sorts nothing; make it at start-up, outside any
+ * stream capture, so that later calls allocate nothing.
+ * The call is synchronous: it reads the sort's error word back and waits for
+ * the stream. It must never be made while its stream (or, in global capture
+ * mode, any stream) is capturing; a capturing stream is rejected with
+ * GS_EINVAL and the capture is left intact. Calls share the array, so calls
+ * whose work overlaps on the GPU race: serialize them. Returns after the
+ * stream has finished the sort. */
 int gs_radix_sort_indices_noalloc(const uint32_t* d_codes, uint32_t N, uint32_t* d_perm,
                                   void* stream);
 

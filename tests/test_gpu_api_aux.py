@@ -9,11 +9,13 @@
 * The walk's interaction counters (gs_counters) agree with the FP64 walk of the
   same acceptance rule on the same tree, up to the few borderline acceptances
   that FP32 and FP64 decide differently; reset returns and clears them.
-* gs_sync waits for queued work, bounded by a timeout.
+* gs_sync waits for queued work, bounded by a timeout; a wait that times out
+  leaves the queued work and the context intact.
 """
 import numpy as np
 import pytest
 
+from galaxy_sim_b200 import _lib
 from galaxy_sim_b200 import initial_conditions as ic
 from galaxy_sim_b200.nbody_gpu import NBodyGPU
 from galaxy_sim_b200.simulation import Physics, Simulation, params_dict
@@ -89,6 +91,22 @@ def test_sync_waits_for_queued_steps(gpu_lib):
     assert sim.stream != 0
     sim.run(20, False)
     sim.sync(timeout_ns=10_000_000_000)  # returns once the 20 steps are done
+    P, _ = sim.readState()
+    assert np.all(np.isfinite(P)) and sim.deviceErrors() == 0
+    sim.destroy()
+
+
+def test_sync_timeout_leaves_the_context_usable(gpu_lib):
+    """A bounded host wait that expires returns GS_ETIMEDOUT without touching the
+    queued work; a later wait sees it finish with no device error."""
+    g = ic.disk_16k()
+    sim = NBodyGPU(0, g.particles, g.stellar)
+    sim.updateParams(dt=0.005, G=1.0, epsilon=0.05, theta=0.5)
+    sim.run(2000, False)                       # about half a second of queued steps
+    with pytest.raises(_lib.GalaxyError) as e:
+        sim.sync(timeout_ns=1)
+    assert e.value.code == _lib.GS_ETIMEDOUT
+    sim.sync(timeout_ns=60_000_000_000)
     P, _ = sim.readState()
     assert np.all(np.isfinite(P)) and sim.deviceErrors() == 0
     sim.destroy()

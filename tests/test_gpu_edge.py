@@ -188,3 +188,24 @@ def test_uploaded_dag_walk_is_bounded(gpu_lib):
         assert ctx.deviceErrors() == 0
         ctx.destroy()
     assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+
+
+def test_sort_lookback_wait_runs_out_and_reports(gpu_lib, oracle):
+    """The sort's look-back is the one device-side wait. With a short test limit
+    and one tile that never publishes its digit counts (a flag that nothing
+    sets), the waits of the tiles after it run out: the kernel returns, the call
+    reports GS_EDEVICE with the look-back bit, and the next sort is correct."""
+    L = gpu_lib
+    codes = np.random.default_rng(17).integers(0, 1 << 30, 12 * 4096 + 5, dtype=np.uint32)
+    perm = np.zeros(codes.size, np.uint32)
+    want = oracle.radix_sort_indices(codes)
+    assert L.gs_test_sort_lookback(0, -1) == _lib.GS_EINVAL
+    assert L.gs_test_sort_lookback(4096, 2) == 0
+    try:
+        rc = L.gs_radix_sort_indices(codes.ctypes.data, codes.size, perm.ctypes.data)
+    finally:
+        assert L.gs_test_sort_lookback(1 << 20, -1) == 0
+    assert rc == _lib.GS_EDEVICE, L.gs_last_error(None)
+    assert b"0x1" in L.gs_last_error(None)
+    assert L.gs_radix_sort_indices(codes.ctypes.data, codes.size, perm.ctypes.data) == 0
+    assert np.array_equal(perm, want)
