@@ -149,6 +149,20 @@ class GalaxyPool:
         self._ok(lib().gs_device_errors(self._ctx, C.byref(b), int(bool(clear))))
         return b.value
 
+    def set_debug(self, enable: bool = True):
+        """Keep each walk's pair forces and leaf densities (read_forces), for every galaxy."""
+        self._ok(lib().gs_set_debug(self._ctx, int(bool(enable))))
+
+    def read_forces(self, slot: int):
+        """{ax, ay, az, phi} per particle (G applied, halo excluded) and own-leaf
+        densities of the last walk of one galaxy; needs set_debug(True) first."""
+        self._sel(slot)
+        N = self.n[slot]
+        acc = np.zeros((N, 4), np.float32)
+        dens = np.zeros(N, np.float32)
+        self._ok(lib().gs_read_forces(self._ctx, ptr(acc), ptr(dens)))
+        return acc, dens
+
     # -- the NBodyGPU surface on one slot ------------------------------------------------------
     def apply_permutation(self, slot: int, perm):
         """NBodyGPU.applyPermutation on one galaxy (out[i] = in[perm[i]], galaxy-local)."""

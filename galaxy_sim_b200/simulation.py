@@ -47,6 +47,27 @@ WORKLOADS = {
 }
 
 
+def batch96(seed: int = 7) -> list:
+    """The batched-ensemble workload: 96 disks with N log-uniform in [4096, 262144],
+    Q uniform in [1, 2], 2-4 arms, gas fraction 0 or 0.3 (gas: drag + star
+    formation), eps 0.02, theta 0.5, dt 0.005. Returns (Galaxy, Physics) pairs."""
+    import math
+
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(96):
+        N = int(round(math.exp(rng.uniform(math.log(4096), math.log(262144)))))
+        Q = float(rng.uniform(1.0, 2.0))
+        arms = int(rng.integers(2, 5))
+        gas = float(rng.choice([0.0, 0.3]))
+        g = ic.galaxy_disk(N, 1000 + k, Q=Q, arms=arms, gas_frac=gas)
+        ph = Physics(0.02, 0.5, 0.005, gas_drag=0.25 if gas else 0.0, sf_eff=0.02 if gas else 0.0)
+        out.append((g, ph))
+    return out
+
+
 def params_dict(galaxy: "ic.Galaxy", ph: Physics, time: float = 0.0) -> dict:
     """NBodyGPU.updateParams arguments for a galaxy (main.js:414-427)."""
     return dict(dt=ph.dt, G=ph.G, epsilon=ph.epsilon, theta=ph.theta,

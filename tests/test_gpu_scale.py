@@ -1,0 +1,170 @@
+"""Parity at the sizes the batched, served and long-run numbers are quoted at.
+
+* The batched ensemble: the seeded 96-galaxy set (N log-uniform in [4096,
+  262144], 4.65 M particles, gas with drag and star formation in about half of
+  them) stepped as one pool. Every galaxy equals its solo run bit for bit. For
+  eight galaxies, the largest included, the pool's own rebuild equals the
+  oracle's sortAndBuild (permutation and topology bit-exact) and the pool's
+  forces fall within the tolerance of the FP64 walk of the same acceptance rule
+  on that tree.
+* The served stream: requests drawn from the served ranges (a disk of 2^20, the
+  collision and sphere presets, eps/theta/dt from their sets) pushed through a
+  continuous-batching server too small to hold them at once. Every result
+  equals the same request run alone, bit for bit.
+* The long run: 1000 steps of the disk of N = 524288 with gas drag and star
+  formation. The device's energy drift follows the oracle's FP32 run of the
+  reference scheme on the same initial conditions (a committed trajectory,
+  tests/golden/drift_disk512k.json, made by tests/golden/make_drift_golden.py).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from galaxy_sim_b200.nbody_gpu import NBodyGPU
+from galaxy_sim_b200.pool import GalaxyPool
+from galaxy_sim_b200.serve import BatchServer, make_request
+from galaxy_sim_b200.simulation import WORKLOADS, Physics, Simulation, batch96, params_dict
+
+pytestmark = pytest.mark.gpu
+
+MED_TOL, P99_TOL = 2e-5, 1e-3   # median and 99th percentile of |da|/|a| against the FP64 walk
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _same(a, b):
+    return np.array_equal(np.asarray(a).view(np.uint32), np.asarray(b).view(np.uint32))
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b, axis=1) / np.maximum(np.linalg.norm(b, axis=1), 1e-30)
+
+
+def _topology_diff(got, want):
+    for f in ("isLeaf", "first", "count", "children", "size"):
+        if not np.array_equal(got[f], want[f]):
+            return f
+    return None
+
+
+def test_batch96_pool_equals_solo_and_forces_within_tolerance(gpu_lib, oracle):
+    gals = batch96()
+    steps = 3
+    pool = GalaxyPool(sum((g.N + 255) // 256 * 256 for g, _ in gals), len(gals))
+    slots = [pool.add(g.particles, g.stellar, params_dict(g, ph), star_formation=ph.sf_eff > 0)
+             for g, ph in gals]
+    assert None not in slots
+    pool.run(steps, True)
+    for (g, ph), s in zip(gals, slots):
+        solo = NBodyGPU(0, g.particles, g.stellar)
+        solo.updateParams(**params_dict(g, ph))
+        solo.run(steps, ph.sf_eff > 0)
+        SP, SS = solo.readState()
+        se = solo.energy()
+        solo.destroy()
+        P, S = pool.read_state(s)
+        assert _same(P, SP) and _same(S, SS), f"galaxy {s} (N={g.N}) differs from its solo run"
+        assert pool.energy(s) == se, s
+        assert pool.device_errors(s) == 0, s
+
+    # forces of eight galaxies on the pool's own rebuild, the largest included
+    order = np.argsort([g.N for g, _ in gals])
+    chosen = sorted({int(order[k]) for k in np.linspace(0, len(gals) - 1, 8).round().astype(int)})
+    assert int(order[-1]) in chosen
+    before = {k: pool.read_state(slots[k]) for k in chosen}
+    pool.set_debug(True)
+    pool.sort_build()
+    trees = {k: pool.get_tree(slots[k]) for k in chosen}
+    sorted_state = {k: pool.read_state(slots[k])[0] for k in chosen}
+    pool.step()
+    worst = []
+    for k in chosen:
+        g, ph = gals[k]
+        acc4, _ = pool.read_forces(slots[k])
+        nodes, lr, perm = trees[k]
+        P0, S0 = before[k]
+        want = oracle.sort_and_build(P0, S0)
+        assert np.array_equal(perm, want["perm"]), k
+        assert _topology_diff(nodes, want["nodes"]) is None, (k, _topology_diff(nodes, want["nodes"]))
+        assert np.array_equal(lr, want["levelRanges"]), k
+        P = sorted_state[k]
+        assert np.array_equal(P, want["sorted"]), k
+        com64 = oracle.refresh_f64(P, want["nodes"], want["levelRanges"])
+        p = oracle.make_params(g.N, epsilon=ph.epsilon, theta=ph.theta, dt=ph.dt)
+        acc64, pot64, _, _ = oracle.walk_f64(p, P, want["nodes"], com64)
+        rel = _rel(acc4[:, :3].astype(np.float64), acc64)
+        relp = np.abs(acc4[:, 3] - pot64) / np.abs(pot64)
+        med, p99 = float(np.median(rel)), float(np.percentile(rel, 99))
+        worst.append((g.N, med, p99))
+        assert med <= MED_TOL and p99 <= P99_TOL, (g.N, med, p99)
+        assert np.median(relp) <= MED_TOL, g.N
+    print("\nbatch96 forces vs FP64 walk (N, median, p99): " +
+          ", ".join(f"({n}, {m:.1e}, {q:.1e})" for n, m, q in worst))
+    pool.close()
+
+
+def _served_requests():
+    specs = [  # preset, N, eps, theta, dt, steps
+        ("disk", 1 << 20, 0.02, 0.5, 0.005, 24),
+        ("collision", 300000, 0.05, 0.7, 0.0025, 31),
+        ("sphere", 200000, 0.02, 0.7, 0.005, 17),
+        ("disk", 8192, 0.05, 0.5, 0.0025, 40),
+        ("collision", 60000, 0.02, 0.5, 0.005, 12),
+        ("sphere", 500000, 0.05, 0.5, 0.005, 20),
+        ("disk", 33000, 0.02, 0.7, 0.0025, 35),
+        ("collision", 1 << 19, 0.02, 0.5, 0.0025, 15),
+    ]
+    return [make_request(rid, 0.01 * rid, preset, N, 5000 + rid, Physics(eps, th, dt), steps)
+            for rid, (preset, N, eps, th, dt, steps) in enumerate(specs)]
+
+
+def test_served_stream_at_request_scale_equals_alone(gpu_lib):
+    reqs = _served_requests()
+    srv = BatchServer(capacity=1_700_000, max_galaxies=4)
+    stats = srv.serve(reqs)
+    srv.close()
+    assert all(r.result is not None for r in reqs)
+    assert stats["particle_steps"] == sum(r.N * r.steps for r in reqs)
+    assert max(r.admitted - r.arrival for r in reqs) > 0     # the pool could not hold them all
+    for r in reqs:
+        sim = NBodyGPU(0, r.particles, r.stellar)
+        sim.updateParams(**r.params)
+        if r.tracking is not None:
+            sim.setTracking(*r.tracking)
+        sim.run(r.steps, r.star_formation)
+        P, S = sim.readState()
+        e = sim.energy()
+        assert sim.deviceErrors() == 0
+        sim.destroy()
+        RP, RS, re_ = r.result
+        assert _same(RP, P) and _same(RS, S), (r.rid, r.preset, r.N)
+        assert re_ == e, (r.rid, r.preset, r.N)
+
+
+def test_energy_drift_1000_steps_at_full_size_follows_the_oracle(gpu_lib):
+    with open(os.path.join(HERE, "golden", "drift_disk512k.json")) as f:
+        ref = json.load(f)
+    w = WORKLOADS[ref["workload"]]
+    rec = {int(k): (ed, et) for k, ed, et in ref["records"]}
+    sim = Simulation(w.make(), w.physics)
+    assert sim.N == ref["N"]
+    got = {}
+    done = 0
+    for k in sorted(rec):
+        sim.run(k - done)
+        done = k
+        e = sim.gpu.energy()
+        got[k] = (e["e_diag"], e["e_true"])
+    assert sim.gpu.deviceErrors() == 0
+    sim.close()
+    first = min(rec)
+    dev = {c: [(got[k][c] - got[first][c]) / abs(got[first][c]) for k in sorted(rec)] for c in (0, 1)}
+    want = {c: [(rec[k][c] - rec[first][c]) / abs(rec[first][c]) for k in sorted(rec)] for c in (0, 1)}
+    print(f"\ndrift over {ref['steps']} steps: device true {dev[1][-1]:+.4e} diag {dev[0][-1]:+.4e}; "
+          f"oracle true {want[1][-1]:+.4e} diag {want[0][-1]:+.4e}")
+    # the whole trajectory, not only its end: at every recorded step the device's
+    # drift stays within 2e-3 (absolute) plus 10% of the oracle's
+    for c in (0, 1):
+        for a, b in zip(dev[c], want[c]):
+            assert abs(a - b) <= 2e-3 + 0.1 * abs(b), (c, a, b)
