@@ -15,9 +15,12 @@ ranks' particle-steps / the slowest rank's device time.
 Timing: W untimed warm-up steps, then K steps, each bracketed by CUDA events on
 the context's stream, with a 256 MiB L2 flush (2x the 126 MB L2) between steps;
 barrier + synchronize on both sides; max over ranks. ``e2e`` is the same
-metric through the C ABI with pinned host buffers: upload of the initial
-state, per step a Params upload and an energy-diagnostic readback, and a final
-state readback, all inside the event-timed region.
+metric through the C ABI with pinned host buffers, frame by frame as main.js
+drives NBodyGPU at one step per frame: upload of the initial state, per step a
+Params upload, the step, the energy-diagnostic readback and the position
+readback (16 B per particle), and a final state readback, all inside the
+event-timed region. ``precision_modes`` gives the step time of the compensated
+walk and of the FP64 internal-node COM refresh on the same workload.
 
 The same line carries the metric's batched and served halves (one GPU):
 ``batched`` = 96 disks (N log-uniform in [4096, 262144]) stepped as one pool,
@@ -25,7 +28,8 @@ one CUDA graph per step, against the same galaxies run back to back in plain
 single-galaxy contexts; ``served`` = a seeded Poisson stream of simulation
 requests (disk / sphere / collision presets, N log-uniform in [8192, 2^20])
 through the continuous-batching server and through a one-at-a-time server,
-with per-step and per-request p50/p99 latency and admission queue wait.
+with per-step and per-request p50/p99 latency and admission queue wait, the
+ratio's upper bound for that mix, and a sweep over arrival rates 1/10/50 per s.
 ``--workload batch96`` and ``--workload serve`` print those alone.
 
 ``--impl reference`` times the reference algorithm on the host cores: the CPU
@@ -47,7 +51,6 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s at N=500k \u03b8=0.5; batched/served vs plain, p50/p99, same GPU"
-WALK_PROFILE = os.path.join(ROOT, "profiles", "walk_kernel_disk512k.md")
 UNIT = "particle-steps/s"
 FLOPS_PER_INTERACTION = 23
 L2_FLUSH_BYTES = 256 << 20
@@ -66,6 +69,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched/served comparison")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch knobs")
+    ap.add_argument("--no-modes", action="store_true", help="skip the precision modes' step times")
+    ap.add_argument("--no-sweep", action="store_true", help="serve: skip the arrival-rate sweep")
     ap.add_argument("--requests", type=int, default=16, help="serve: requests in the stream")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrival rate (1/s)")
     ap.add_argument("--min-steps", type=int, default=100, help="serve: fewest steps of a request")
@@ -117,12 +122,12 @@ def workload(args):
     return w
 
 
-def config_of(w, g, args, l2="flush 256 MiB between timed steps"):
+def config_of(w, g, args):
     ph = w.physics
     return {"workload": w.name, "N": int(g.N), "theta": ph.theta, "epsilon": ph.epsilon,
             "dt": ph.dt, "gas_drag": ph.gas_drag, "sf_eff": ph.sf_eff, "bucket": 16,
             "morton_bits": 30, "precision": "fp32 walk, fp32 COM refresh",
-            "parallelism": f"replicas x{args.gpus} (no collective)", "l2": l2}
+            "parallelism": f"replicas x{args.gpus} (no collective)"}
 
 
 class Clocks:
@@ -276,9 +281,25 @@ def run_ours(args, ws, rank, local):
                                f"{FLOPS_PER_INTERACTION} flops per launch",
                 "walk_ms": round(walk_avg, 4), "walk_ms_mean": round(sum(walk_ms) / R, 4),
                 "walk_samples": R, "sort_build_refresh_ms": round(statistics.median(build_ms), 4),
-                "traffic": walk_traffic(w.name, w.physics.theta),
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch "
-                                  "(profiles/walk_kernel_disk512k.md)"}
+                "traffic": None,
+                "traffic_note": "DRAM bytes per launch come from an ncu capture of the same kernel, "
+                                "not from this run (no DRAM counter is read at bench time)"}
+
+    # ---- the precision modes' step time (same workload, same timing) ----
+    precision = None
+    if not args.no_modes:
+        precision = {}
+        for name, comp, com in (("fp32", 0, 0), ("compensated", 1, 0), ("com64", 0, 2), ("both", 1, 2)):
+            sim.gpu.setWalkMode(bool(comp))
+            sim.gpu.setComMode(com)
+            sim.run(3)
+            t = _timed_steps(sim.gpu.stream, local, 20, lambda: sim.run(1), flush)
+            precision[name] = round(statistics.median(t), 4)
+        sim.gpu.setWalkMode(False)
+        sim.gpu.setComMode(0)
+        precision["unit"] = "ms per full step, median of 20 (L2 flushed between steps)"
+        precision["modes"] = {"fp32": "FP32 walk, FP32 COM", "compensated": "Kahan far-field sums",
+                              "com64": "FP64 internal-node COM", "both": "Kahan sums + FP64 COM"}
 
     # ---- e2e through the C ABI with pinned host buffers ----
     e2e = None
@@ -290,7 +311,7 @@ def run_ours(args, ws, rank, local):
         hs = torch.from_numpy(g.stellar.reshape(-1)).pin_memory()
         outp = torch.empty(N * 8, dtype=torch.float32).pin_memory()
         outs = torch.empty(N * 4, dtype=torch.float32).pin_memory()
-        prm = _lib.GsParams()
+        outpos = torch.empty(N * 4, dtype=torch.float32).pin_memory()
         pd = params_dict(g, w.physics)
         sim.gpu.updateParams(**pd)
         prm = sim.gpu._params
@@ -306,22 +327,27 @@ def run_ours(args, ws, rank, local):
             e0.record(ext)
         _lib.check(L.gs_write_state(ctx, hp.data_ptr(), hs.data_ptr()), ctx)
         for k in range(Ke):
-            prm.time = k * w.physics.dt   # main.js passes simTime with every updateParams
+            # one frame of main.js:400-507 at one step per frame: Params with the
+            # clock, the step (rebuild on the device), the HUD's energy and the
+            # frame's position readback (vec4 pos + e_i per particle)
+            prm.time = k * w.physics.dt
             _lib.check(L.gs_update_params(ctx, C.byref(prm)), ctx)
             _lib.check(L.gs_run(ctx, 1, int(sim.star_formation)), ctx)
             _lib.check(L.gs_energy(ctx, C.byref(diag)), ctx)
+            _lib.check(L.gs_read_positions(ctx, outpos.data_ptr(), 0), ctx)
         _lib.check(L.gs_read_state(ctx, outp.data_ptr(), outs.data_ptr()), ctx)
         with torch.cuda.stream(ext):
             e1.record(ext)
         torch.cuda.synchronize()
         te_ms = rank_max(dist, e0.elapsed_time(e1), f"cuda:{local}")
-        if not np.isfinite(diag.e_diag):
-            raise RuntimeError("non-finite energy diagnostic in the e2e run")
+        if not np.isfinite(diag.e_diag) or not bool(torch.isfinite(outpos).all()):
+            raise RuntimeError("non-finite energy or positions in the e2e run")
         e2e = {"value": round(job_value(N * Ke, ws, te_ms), 1), "unit": UNIT,
                "h2d_bytes_per_step": int(round((N * 48 + Ke * 96) / Ke)),
-               "d2h_bytes_per_step": int(round((Ke * 48 + N * 48) / Ke)),
-               "path": "gs_write_state (pinned) + K x [gs_update_params, gs_run(1), gs_energy] "
-                       "+ gs_read_state (pinned)", "steps": Ke, "ms": round(te_ms, 3)}
+               "d2h_bytes_per_step": int(round((Ke * (48 + 16 * N) + N * 48) / Ke)),
+               "path": "gs_write_state (pinned) + K frames of [gs_update_params, gs_run(1), gs_energy, "
+                       "gs_read_positions (pinned, 16 B/particle)] + gs_read_state (pinned)",
+               "steps": Ke, "ms": round(te_ms, 3)}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -332,7 +358,9 @@ def run_ours(args, ws, rank, local):
         # the metric's batched/served halves: 96 galaxies in one pool vs back-to-back
         # plain runs, and a Poisson request stream through both servers
         batched = batch_compare(local, min(K, 100), max(3, min(args.warmup, 5)))
-        served = serve_compare(local, args.requests, args.rate, args.min_steps, args.max_steps)
+        served = serve_compare(local, args.requests, args.rate, args.min_steps, args.max_steps,
+                               rate_ceiling=(value, batched["value"]),
+                               sweep=() if args.no_sweep else (1.0, 10.0, 50.0))
     if dist:
         dist.destroy_process_group()
     if rank != 0:
@@ -342,12 +370,13 @@ def run_ours(args, ws, rank, local):
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": ws, "steps": K,
         "warmup": args.warmup, "ms_per_step": round(max_ms / K, 5), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ICs)",
-        "config": config_of(w, g, args),
+        "config": config_of(w, g, args), "l2": "flush 256 MiB between timed steps",
         "latency_ms": {"p50": round(step_sorted[len(step_sorted) // 2], 5),
                        "p99": round(step_sorted[min(len(step_sorted) - 1, int(0.99 * len(step_sorted)))], 5),
                        "max": round(step_sorted[-1], 5)},
         "interactions_per_particle": round(interactions / N, 2),
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+        "precision_modes": precision,
         "gpu_launches": K * n_launch_step,
         "batched": batched, "served": served, "autotune": tuned,
     }
@@ -404,7 +433,7 @@ def run_reference(args, ws, rank, local):
         "warmup": args.warmup, "ms_per_step": round(1e3 * g.N / cpu["value"], 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded ICs)", "impl": "reference",
-        "config": config_of(w, g, args, l2="host run"),
+        "config": config_of(w, g, args), "l2": "host run (no device caches involved)",
         "cpu_baseline": cpu,
         "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -435,20 +464,6 @@ def _timed_steps(stream_ptr, local, K, step, flush):
             ev[k][1].record(ext)
     torch.cuda.synchronize()
     return [a.elapsed_time(b) for a, b in ev]
-
-
-def walk_traffic(workload: str, theta: float):
-    """DRAM bytes per walk launch from the committed ncu summary (disk512k, theta 0.5)."""
-    import re
-
-    if workload != "disk512k" or theta != 0.5:
-        return None
-    try:
-        m = re.search(r"dram__bytes_read.sum \+ dram__bytes_write.sum \| ([0-9.]+) MB \+ ([0-9.]+) MB",
-                      open(WALK_PROFILE).read())
-    except OSError:
-        return None
-    return int(round((float(m.group(1)) + float(m.group(2))) * 1e6)) if m else None
 
 
 def batch_compare(local, K, W, tune=True):
@@ -512,29 +527,53 @@ def batch_compare(local, K, W, tune=True):
     }
 
 
-def serve_compare(local, n_req, rate, min_steps, max_steps):
+def serve_compare(local, n_req, rate, min_steps, max_steps, rate_ceiling=(), sweep=()):
     """Served stream (Poisson arrivals) through the continuous-batching server
-    and through the one-at-a-time server on the same GPU."""
+    and through the one-at-a-time server on the same GPU.
+
+    ``ratio_bound`` is the largest served/plain ratio this mix allows: no server
+    can finish the mix's particle-steps faster than the GPU's best measured
+    per-particle rate (``rate_ceiling``: the batched server's own device rate, or
+    a faster rate measured in the same run), so batched wall time >= particle-steps
+    / ceiling and the ratio <= plain wall time x ceiling / particle-steps.
+    ``sweep`` repeats the comparison at other arrival rates (half the requests)."""
     import torch
 
     from galaxy_sim_b200.serve import BatchServer, PlainServer, make_stream
 
     torch.cuda.set_device(local)
-    reqs = make_stream(n_req, rate, seed=11, step_range=(min_steps, max_steps))
-    srv = BatchServer(max_galaxies=64, device=local)
-    with Clocks(local) as clk:
-        b = srv.serve(reqs)
-    clocks = clk.summary()
-    srv.close()
-    reqs2 = make_stream(n_req, rate, seed=11, step_range=(min_steps, max_steps))
-    p = PlainServer(local).serve(reqs2)
+
+    def both(n, r):
+        reqs = make_stream(n, r, seed=11, step_range=(min_steps, max_steps))
+        srv = BatchServer(max_galaxies=64, device=local)
+        with Clocks(local) as clk:
+            b = srv.serve(reqs)
+        srv.close()
+        reqs2 = make_stream(n, r, seed=11, step_range=(min_steps, max_steps))
+        p = PlainServer(local).serve(reqs2)
+        return b, p, clk.summary()
+
+    b, p, clocks = both(n_req, rate)
+    ps = b["particle_steps"]
+    ceiling = max([ps / b["gpu_busy_s"]] + [x for x in rate_ceiling if x])
+    bound = {"value": round(p["wall_s"] * ceiling / ps, 3), "rate_ceiling": round(ceiling, 1),
+             "plain_wall_s": p["wall_s"], "plain_device_s": p["gpu_busy_s"],
+             "batched_wall_s": b["wall_s"], "batched_device_s": b["gpu_busy_s"],
+             "particle_steps": ps}
+    rows = []
+    for r in sweep:
+        n = max(4, n_req // 2)
+        sb, sp, _ = both(n, r)
+        rows.append({"rate_per_s": r, "requests": n, "batched": sb["value"], "plain": sp["value"],
+                     "batched_over_plain": round(sb["value"] / sp["value"], 3),
+                     "batched_step_ms_p50": sb["step_ms"]["p50"], "batched_step_ms_p99": sb["step_ms"]["p99"]})
     return {"value": b["value"], "unit": UNIT,
             "config": {"workload": "serve", "requests": n_req, "rate_per_s": rate,
                        "N_range": [8192, 1 << 20], "steps_range": [min_steps, max_steps],
                        "presets": ["disk", "sphere", "collision"], "eps": [0.02, 0.05],
                        "theta": [0.5, 0.7], "dt": [0.0025, 0.005]},
             "batched": b, "plain": p, "batched_over_plain": round(b["value"] / p["value"], 3),
-            "clocks": clocks}
+            "ratio_bound": bound, "rate_sweep": rows, "clocks": clocks}
 
 
 def _mode_line(d):
@@ -553,7 +592,8 @@ def run_batch(args, ws, rank, local):
 def run_serve(args, ws, rank, local):
     if rank != 0:
         return
-    d = serve_compare(local, args.requests, args.rate, args.min_steps, args.max_steps)
+    d = serve_compare(local, args.requests, args.rate, args.min_steps, args.max_steps,
+                      sweep=() if args.no_sweep else (1.0, 10.0, 50.0))
     print(json.dumps(_mode_line(d)), flush=True)
 
 
