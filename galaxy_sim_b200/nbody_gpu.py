@@ -23,10 +23,11 @@ from ._lib import NODE_DTYPE, GsDiag, GsParams, check, f32, lib, ptr, u32
 def build_params(N, *, dt, G, epsilon, theta=0.5, haloMass=0, haloA=1, gasDrag=0, time=0,
                  agingRate=25, sfDensity=1e9, sfEff=0, sfDt=0, haloCenters=()) -> GsParams:
     """The Params uniform NBodyGPU.updateParams writes (NBodyGPU.js:253-275):
-    epsilon^2 in f32, N forced, at most two halo centres."""
+    epsilon * epsilon in double rounded to f32 (the Float32Array store), N
+    forced, at most two halo centres."""
     p = GsParams()
     p.dt, p.G = dt, G
-    p.epsilon2 = float(np.float32(epsilon) * np.float32(epsilon))
+    p.epsilon2 = float(np.float32(float(epsilon) * float(epsilon)))  # double product, f32 store
     p.N = int(N)
     p.theta, p.haloMass, p.haloA, p.gasDrag = theta, haloMass, haloA, gasDrag
     p.time, p.agingRate, p.sfDensity, p.sfEff, p.sfDt = time, agingRate, sfDensity, sfEff, sfDt

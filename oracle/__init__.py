@@ -88,7 +88,7 @@ def make_params(N, dt=0.005, G=1.0, epsilon=0.05, theta=0.5, haloMass=0.0, haloA
     """Fill Params the way NBodyGPU.updateParams does (NBodyGPU.js:253-275)."""
     p = Params()
     p.dt, p.G = dt, G
-    p.epsilon2 = np.float32(np.float32(epsilon) * np.float32(epsilon))
+    p.epsilon2 = np.float32(float(epsilon) * float(epsilon))   # JS: double product, f32 store
     p.N = N
     p.theta, p.haloMass, p.haloA, p.gasDrag = theta, haloMass, haloA, gasDrag
     p.time, p.agingRate, p.sfDensity, p.sfEff, p.sfDt = time, agingRate, sfDensity, sfEff, sfDt
