@@ -71,6 +71,7 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch knobs")
     ap.add_argument("--no-modes", action="store_true", help="skip the precision modes' step times")
     ap.add_argument("--no-sweep", action="store_true", help="serve: skip the arrival-rate sweep")
+    ap.add_argument("--no-small", action="store_true", help="skip the config-0 (16384-particle) line")
     ap.add_argument("--requests", type=int, default=16, help="serve: requests in the stream")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrival rate (1/s)")
     ap.add_argument("--min-steps", type=int, default=100, help="serve: fewest steps of a request")
@@ -349,6 +350,11 @@ def run_ours(args, ws, rank, local):
                        "gs_read_positions (pinned, 16 B/particle)] + gs_read_state (pinned)",
                "steps": Ke, "ms": round(te_ms, 3)}
 
+    # ---- config 0 (the 16384-particle disk): step and walk time per walk group size ----
+    small = None
+    if ws == 1 and not args.no_small:
+        small = small_disk(local, flush)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(w, g, steps=5, warmup=1, budget_s=15.0)
@@ -376,11 +382,56 @@ def run_ours(args, ws, rank, local):
                        "max": round(step_sorted[-1], 5)},
         "interactions_per_particle": round(interactions / N, 2),
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-        "precision_modes": precision,
+        "precision_modes": precision, "config0": small,
         "gpu_launches": K * n_launch_step,
         "batched": batched, "served": served, "autotune": tuned,
     }
     print(json.dumps(line), flush=True)
+
+
+def small_disk(local, flush, steps=50, warmup=5):
+    """Config 0 (one disk of N = 16384, eps 0.05, theta 0.5, no gas): full-step and
+    walk time at each walk group size, the default (by galaxy size) first."""
+    import torch
+
+    from galaxy_sim_b200 import _lib
+    from galaxy_sim_b200.autotune import set_
+    from galaxy_sim_b200.simulation import WORKLOADS, Simulation
+
+    w = WORKLOADS["disk16k"]
+    g = w.make()
+    out = {"workload": w.name, "N": int(g.N), "theta": w.physics.theta, "epsilon": w.physics.epsilon,
+           "unit": "ms", "by_group": {}}
+    for wg in (0, 8, 16, 32):
+        sim = Simulation(g, w.physics, device=local)
+        set_(sim.gpu._ctx, _lib.TUNE_WALK_GROUP, wg)
+        sim.run(warmup)
+        t = _timed_steps(sim.gpu.stream, local, steps, lambda: sim.run(1), flush)
+        ext = torch.cuda.ExternalStream(sim.gpu.stream, device=torch.device("cuda", local))
+        walk = []
+        for _ in range(10):
+            a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            with torch.cuda.stream(ext):
+                torch.cuda._sleep(GATE_CYCLES // 4)
+                flush.fill_(2.0)
+                a.record(ext)
+            sim.gpu.sortBuild()
+            with torch.cuda.stream(ext):
+                b.record(ext)
+            sim.gpu.step()
+            with torch.cuda.stream(ext):
+                c.record(ext)
+            sim.sync()
+            walk.append(b.elapsed_time(c))
+        sim.close()
+        key = "by_size" if wg == 0 else str(wg)
+        out["by_group"][key] = {"ms_per_step": round(statistics.median(t), 4),
+                                "walk_ms": round(statistics.median(walk), 4)}
+    d = out["by_group"]["by_size"]
+    out["ms_per_step"], out["walk_ms"] = d["ms_per_step"], d["walk_ms"]
+    out["value"] = round(g.N / (d["ms_per_step"] / 1e3), 1)
+    out["walk_group"] = "by galaxy size (8 particles at N = 16384)"
+    return out
 
 
 def cpu_baseline(w, g, steps, warmup, budget_s, nthreads=0):

@@ -106,7 +106,7 @@ uint64_t plan_bytes(const Plan& p) {
   b += n * (16 + 16 + 4 + 4 + 4 + 1 + 4) + 4;   // cm, info, node_start, child_base, parent, depth, arrive
   b += s * (sizeof(DevState) + sizeof(TreeMeta) + sizeof(MortonFrame) + 4 + kPartials * 8 + sizeof(SegDesc));
   b += (uint64_t)(p.sort_tiles + p.flag_tiles + p.groups) * 4;
-  b += (uint64_t)p.groups * kPartials * 8 + 16;
+  b += (uint64_t)p.groups * kWalkParts * kPartials * 8 + 16;
   b += (uint64_t)p.diag_chunks * kPartials * 8 + s * 4;
   return b;
 }
@@ -221,7 +221,7 @@ struct gs_ctx {
   // walk
   double* partials = nullptr;
   unsigned* walk_work = nullptr;
-  uint32_t walk_grid = 0;
+  uint32_t walk_grid = 0;   // persistent walk grid (largest class)
   float4* dbg_acc = nullptr;
   float* dbg_dens = nullptr;
   bool debug = false;
@@ -235,6 +235,8 @@ struct gs_ctx {
   int com_mode = kComF32;
   int sort_items = kSortItems;     // tuning: keys per thread of a sort tile (8 or 16)
   int walk_bps = kWalkBlocksPerSM; // tuning: persistent walk blocks per SM (1..8; < 8: 72-register build)
+  int walk_group = 0;              // tuning: walk group size (0: by galaxy size; 8, 16 or 32 particles)
+  uint32_t walk_items[3] = {0, 0, 0};  // work items of the layout per lanes-per-particle class (1, 2, 4)
   bool walk_comp = false;  // Kahan-compensated far-field sums in the walk
   void* host_stage = nullptr;  // pinned: [slots] params
   std::map<int, cudaGraphExec_t> graphs;
@@ -363,7 +365,7 @@ int pool_init(gs_ctx* c, int device, uint64_t cap, uint32_t slots) {
   A(c->sort_map, p.sort_tiles);
   A(c->flag_map, p.flag_tiles);
   A(c->group_map, p.groups);
-  A(c->partials, (size_t)p.groups * kPartials);
+  A(c->partials, (size_t)p.groups * kWalkParts * kPartials);
   A(c->walk_work, 4);
 #undef A
   CK(c, cudaMemset(c->seg_ctr, 0, sizeof(unsigned) * p.slots), "memset");
@@ -374,7 +376,7 @@ int pool_init(gs_ctx* c, int device, uint64_t cap, uint32_t slots) {
   CK(c, cudaMemset(c->st, 0, sizeof(DevState) * p.slots), "memset");
   CK(c, cudaMemset(c->diag_out, 0, sizeof(double) * kPartials * p.slots), "memset");
   CK(c, cudaMemset(c->diag_ctr, 0, sizeof(unsigned) * p.slots), "memset");
-  CK(c, cudaMemset(c->partials, 0, sizeof(double) * kPartials * p.groups), "memset");
+  CK(c, cudaMemset(c->partials, 0, sizeof(double) * kPartials * kWalkParts * p.groups), "memset");
   CK(c, cudaMemset(c->walk_work, 0, 16), "memset");
   CK(c, cudaMallocHost(&c->host_stage, sizeof(gs_params) * (size_t)p.slots + 256), "pinned stage");
   c->slots.assign(p.slots, Slot());
@@ -397,6 +399,18 @@ void pool_release(gs_ctx* c) {
   c->stream = nullptr;
 }
 
+// Walk lanes per particle of a galaxy of n particles: the context's forced group
+// size, or by size (a small galaxy walks in groups of 8 or 16 particles so that
+// its walk fills more warps).
+uint32_t walk_lpp(const gs_ctx* c, uint32_t n) {
+  if (c->walk_group == 8) return 4;
+  if (c->walk_group == 16) return 2;
+  if (c->walk_group == 32) return 1;
+  if (n <= kWalkAuto8) return 4;
+  if (n <= kWalkAuto16) return 2;
+  return 1;
+}
+
 // Rebuild the device layout (galaxies in offset order, tile/group maps) after
 // slots were added or removed. The stream must be idle (no step in flight).
 int ensure_layout(gs_ctx* c) {
@@ -408,6 +422,7 @@ int ensure_layout(gs_ctx* c) {
             [&](uint32_t a, uint32_t b) { return c->slots[a].off < c->slots[b].off; });
   std::vector<SegDesc> h(order.size());
   uint32_t st = 0, ft = 0, gr = 0, dc = 0, hs = 0;
+  uint32_t items[3] = {0, 0, 0};
   for (size_t r = 0; r < order.size(); r++) {
     Slot& s = c->slots[order[r]];
     s.rank = (uint32_t)r;
@@ -423,10 +438,12 @@ int ensure_layout(gs_ctx* c) {
     d.max_nodes = s.max_nodes ? s.max_nodes : 2 * s.n + 4096;
     d.slot = order[r];
     d.diag_chunk0 = dc;
+    d.wlpp = walk_lpp(c, s.n);
     h[r] = d;
     dc += cdiv(cdiv(s.n, kWalkGroup), kDiagChunk);
     st += cdiv(s.n, (uint64_t)kSortThreads * c->sort_items);
     ft += cdiv(s.n, kFlagTile);
+    items[h[r].wlpp == 1 ? 0 : h[r].wlpp == 2 ? 1 : 2] += cdiv(s.n, kWalkGroup) * h[r].wlpp;
     gr += cdiv(s.n, kWalkGroup);
     hs = std::max(hs, order[r] + 1);
   }
@@ -453,7 +470,9 @@ int ensure_layout(gs_ctx* c) {
   L.diag_chunks = dc;
   c->hist_slots = hs;
   c->seg_host = h;
-  c->walk_grid = std::min<uint32_t>(cdiv(gr, kWalkWarps), (uint32_t)c->sms * c->walk_bps);
+  const uint32_t most = std::max(items[0], std::max(items[1], items[2]));
+  c->walk_grid = std::min<uint32_t>(std::max<uint32_t>(1, cdiv(most, kWalkWarps)), (uint32_t)c->sms * c->walk_bps);
+  for (int k = 0; k < 3; k++) c->walk_items[k] = items[k];
   c->drop_graphs();
   c->lay_dirty = false;
   return GS_OK;
@@ -523,11 +542,11 @@ void enqueue_build(gs_ctx* c, const float4* pos, uint32_t stride, int com_mode, 
     launch_pdl(tree_leaves_kernel<kComF32>, L.flag_tiles, kLeafThreads, s, b, L, pos, stride, c->st);
 }
 
-template <int MINB>
+template <int MINB, int LPP>
 void launch_walk(int v, uint32_t g, cudaStream_t s, const WalkArgs& a) {
   switch (v) {
 #define GS_WALK_CASE(V, SF, DBG, ONE, COMP) \
-  case V: launch_pdl(walk_kernel<SF, DBG, ONE, COMP, MINB>, g, kWalkThreads, s, a); break;
+  case V: launch_pdl(walk_kernel<SF, DBG, ONE, COMP, MINB, LPP>, g, kWalkThreads, s, a); break;
     GS_WALK_CASE(0, false, false, false, false)
     GS_WALK_CASE(1, true, false, false, false)
     GS_WALK_CASE(2, false, true, false, false)
@@ -570,9 +589,16 @@ void enqueue_walk(gs_ctx* c, int sf) {
   if (one) a.seg0 = c->seg_host[0];
   else memset(&a.seg0, 0, sizeof(a.seg0));
   const int v = (sf ? 1 : 0) | (c->debug ? 2 : 0) | (one ? 4 : 0) | (c->walk_comp ? 8 : 0);
-  // 8 blocks per SM: the 64-register build; fewer: the 72-register build
-  if (c->walk_bps >= kWalkBlocksPerSM) launch_walk<kWalkBlocksPerSM>(v, g, s, a);
-  else launch_walk<kWalkBlocksWide>(v, g, s, a);
+  // one launch per walk group size present (a single galaxy: its own); 8 blocks
+  // per SM: the 64-register build, fewer: the 72-register build (groups of 32)
+  for (int k = 0; k < 3; k++) {
+    if (!c->walk_items[k]) continue;
+    const uint32_t gk = std::min<uint32_t>(g, std::max<uint32_t>(1, cdiv(c->walk_items[k], kWalkWarps)));
+    if (k == 1) launch_walk<kWalkBlocksPerSM, 2>(v, gk, s, a);
+    else if (k == 2) launch_walk<kWalkBlocksPerSM, 4>(v, gk, s, a);
+    else if (c->walk_bps >= kWalkBlocksPerSM) launch_walk<kWalkBlocksPerSM, 1>(v, gk, s, a);
+    else launch_walk<kWalkBlocksWide, 1>(v, gk, s, a);
+  }
   // per-galaxy FP64 diagnostics of this walk
   launch_pdl(diag_reduce_kernel, c->lay.diag_chunks, dim3(32, kPartials), s, (const double*)c->partials, c->lay,
              c->diag_chunk, c->diag_ctr, c->diag_out);
@@ -1198,6 +1224,10 @@ int gs_set_tuning(gs_ctx* ctx, int knob, int value) {
   } else if (knob == GS_TUNE_SORT_ITEMS) {
     if (value != 8 && value != 16) return ctx->fail(GS_EINVAL, "sort keys per thread must be 8 or 16");
     ctx->sort_items = value;
+  } else if (knob == GS_TUNE_WALK_GROUP) {
+    if (value != 0 && value != 8 && value != 16 && value != 32)
+      return ctx->fail(GS_EINVAL, "walk group must be 0 (by galaxy size), 8, 16 or 32 particles");
+    ctx->walk_group = value;
   } else {
     return ctx->fail(GS_EINVAL, "unknown tuning knob %d", knob);
   }
@@ -1212,6 +1242,7 @@ int gs_get_tuning(gs_ctx* ctx, int knob, int* value) {
   if (!value) return ctx->fail(GS_EINVAL, "value is NULL");
   if (knob == GS_TUNE_WALK_BLOCKS_PER_SM) *value = ctx->walk_bps;
   else if (knob == GS_TUNE_SORT_ITEMS) *value = ctx->sort_items;
+  else if (knob == GS_TUNE_WALK_GROUP) *value = ctx->walk_group;
   else return ctx->fail(GS_EINVAL, "unknown tuning knob %d", knob);
   return GS_OK;
 }

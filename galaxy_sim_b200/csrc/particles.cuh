@@ -363,7 +363,7 @@ __global__ void upload_convert_kernel(const gs_node* __restrict__ nodes, uint32_
   }
 }
 
-// FP64 diagnostics: fold each galaxy's per-group walk partials into
+// FP64 diagnostics: fold each galaxy's per-item walk partials into
 // out[slot][kPartials]. A block of 32 x kPartials threads sums kDiagChunk groups
 // of one galaxy (chunks counted from the galaxy's first group); the galaxy's
 // last block adds the chunk sums in chunk order, so the result does not depend
@@ -387,7 +387,9 @@ __global__ void __launch_bounds__(32 * kPartials)
   const uint32_t g0 = (x - sd.diag_chunk0) * kDiagChunk, g1 = min(ng, g0 + kDiagChunk);
   const int k = threadIdx.y, lane = threadIdx.x;
   double v = 0;
-  for (uint32_t b = g0 + lane; b < g1; b += 32) v += partials[(size_t)(sd.group0 + b) * kPartials + k];
+  for (uint32_t b = g0 + lane; b < g1; b += 32)
+    for (uint32_t q = 0; q < sd.wlpp; q++)  // the group's work items, in order
+      v += partials[((size_t)(sd.group0 + b) * kWalkParts + q) * kPartials + k];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   if (lane == 0) chunk_part[(size_t)x * kPartials + k] = v;

@@ -19,9 +19,19 @@
 //   * Children are tested two at a time, and an opened leaf's particles are
 //     staged the same way and summed two at a time, with sm_100's packed
 //     FP32x2 FMA/ADD/MUL; accumulation is predicated, not branched.
-//   * Warps are persistent and take 32-particle groups from an atomic counter
-//     (load balance across the dense core); per-group FP64 partials of the
+//   * Warps are persistent and take work items from an atomic counter (load
+//     balance across the dense core); per-item FP64 partials of the
 //     diagnostics replace a block-wide barrier.
+//   * Walk group size: a work item is 32, 16 or 8 Morton-consecutive particles
+//     (LPP = 1, 2 or 4 lanes per particle). With LPP > 1 the lanes of a
+//     particle split the round's slot pairs and each opened leaf's source pairs
+//     between them and add their partial sums by shuffles at the end, so a
+//     small galaxy keeps more warps busy and each warp walks the union of
+//     fewer frontiers. A 32-particle walk group (layout, diagnostics) holds LPP
+//     items. The split changes the order of the force sums, so results change
+//     at the rounding level (inside the force tolerance) between group sizes;
+//     each galaxy carries its own LPP, so it gets the same arithmetic alone or
+//     in a pool.
 //   * Over a batch, every group belongs to one galaxy and walks that galaxy's
 //     tree with its own Params; warps steal groups across all galaxies.
 #pragma once
@@ -43,7 +53,12 @@ constexpr int kWalkStack = 8 * 11 * kWalkRanges;
 // thread) and for 7 (72 registers, fewer spills); the launch tuning picks one.
 constexpr int kWalkBlocksPerSM = 8;
 constexpr int kWalkBlocksWide = 7;
-constexpr uint32_t kWalkGroup = 32;             // particles per warp (one per lane)
+constexpr uint32_t kWalkGroup = 32;             // particles per walk group (layout, diagnostics)
+constexpr uint32_t kWalkParts = 4;              // work items per group in a pool (the largest LPP)
+// galaxies of at most this many particles walk in groups of 8 / 16 particles
+// (the context's default; GS_TUNE_WALK_GROUP forces one size)
+constexpr uint32_t kWalkAuto8 = 24576;
+constexpr uint32_t kWalkAuto16 = 98304;
 
 // nbody_bh.wgsl:206-213
 __device__ inline uint32_t pcg(uint32_t v0) {
@@ -109,7 +124,7 @@ struct WalkArgs {
   float* __restrict__ energy;       // e_i
   float4* __restrict__ dbg_acc;     // optional {ax, ay, az, phi} (G applied)
   float* __restrict__ dbg_dens;
-  double* __restrict__ partials;    // [groups][kPartials]
+  double* __restrict__ partials;    // [groups][kWalkParts][kPartials]
   unsigned* work;                   // [0] next group, [1] finished warps (self-resetting)
   Layout L;                         // galaxies and the group -> galaxy map
   uint32_t pool_n, node_pool;       // particle and node pool sizes (memory-safety bounds)
@@ -128,19 +143,21 @@ struct WalkSmem {
 };
 
 // Direct sum of a staged leaf segment [off, off + k) for the lanes in `me`
-// (nbody_bh.wgsl:117-131), two sources per packed step. With soft (eps^2 > 0)
-// the self pair is included (zero force at r = 0) and its potential removed
-// once at the end of the walk via selfw; otherwise it is skipped per pair.
-template <typename Smem>
+// (nbody_bh.wgsl:117-131), two sources per packed step. A particle served by
+// LPP lanes splits the source pairs: lane `sub` takes pairs sub, sub + LPP, ...
+// With soft (eps^2 > 0) the self pair is included (zero force at r = 0) and its
+// potential removed once at the end of the walk via selfw (counted by the lane
+// whose share holds it); otherwise it is skipped per pair.
+template <int LPP, typename Smem>
 __device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k, uint32_t jself,
                                          bool me, bool soft, float2 px, float2 py, float2 pz,
                                          float eps2, float2& ax, float2& ay, float2& az,
                                          float2& pt, float& selfw, unsigned long long& npair,
-                                         bool dbg) {
+                                         bool dbg, uint32_t sub) {
   if (soft) {
     const float2 wme = make_float2(me ? 1.0f : 0.0f, me ? 1.0f : 0.0f);
-    if (me && jself < k) selfw += 1.0f;
-    for (uint32_t j = 0; j < k; j += 2) {
+    if (me && jself < k && ((jself >> 1) % LPP) == sub) selfw += 1.0f;
+    for (uint32_t j = 2 * sub; j < k; j += 2 * LPP) {
       const float2 jx = *reinterpret_cast<const float2*>(&S.lx[off + j]);
       const float2 jy = *reinterpret_cast<const float2*>(&S.ly[off + j]);
       const float2 jz = *reinterpret_cast<const float2*>(&S.lz[off + j]);
@@ -154,10 +171,10 @@ __device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k
       ay = __ffma2_rn(ey, ff, ay);
       az = __ffma2_rn(ez, ff, az);
       pt = __fadd2_rn(pt, mr);
+      if (dbg && me) npair += (j != jself) + (j + 1 < k && j + 1 != jself);
     }
-    if (dbg && me) npair += k - (jself < k ? 1 : 0);
   } else {
-    for (uint32_t j = 0; j < k; j += 2) {
+    for (uint32_t j = 2 * sub; j < k; j += 2 * LPP) {
       const float2 jx = *reinterpret_cast<const float2*>(&S.lx[off + j]);
       const float2 jy = *reinterpret_cast<const float2*>(&S.ly[off + j]);
       const float2 jz = *reinterpret_cast<const float2*>(&S.lz[off + j]);
@@ -214,22 +231,34 @@ __device__ __forceinline__ uint32_t warp_transpose(uint32_t x, int lane) {
 // contributions are summed with Kahan compensation; near-field leaf sums add
 // plainly into the same sums.
 // MINB: resident blocks per SM the register budget is compiled for.
-template <bool SF, bool DBG, bool ONE, bool COMP, int MINB>
+// LPP: lanes per particle (walk group of 32 / LPP particles); a launch walks the
+// galaxies whose SegDesc wlpp field equals LPP and skips the others' work items.
+template <bool SF, bool DBG, bool ONE, bool COMP, int MINB, int LPP>
 __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
+  static_assert(LPP == 1 || LPP == 2 || LPP == 4, "lanes per particle");
+  constexpr uint32_t G = 32 / LPP;                         // particles per work item
+  constexpr int NPP = 16 / LPP;                            // slot pairs a lane tests in a full round
+  constexpr unsigned GMASK = G == 32 ? 0xffffffffu : (1u << G) - 1u;
+  constexpr uint32_t kStride = ONE ? LPP : kWalkParts;    // work items per walk group
   griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
   __shared__ WalkSmem smem_all[kWalkWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t pl = lane % G;    // the lane's particle within the item
+  const uint32_t sub = lane / G;   // its share of the slot pairs and leaf sources
+  // slots whose pairs this lane tests: pairs sub, sub + LPP, ... (bits 2pp, 2pp + 1)
+  const uint32_t mine = LPP == 1 ? 0xffffffffu : LPP == 2 ? (0x33333333u << (2 * sub)) : (0x03030303u << (2 * sub));
   WalkSmem& S = smem_all[warp];
-  const uint32_t ngroups = a.L.groups;
+  const uint32_t nitems = a.L.groups * kStride;
   const unsigned full = 0xffffffffu;
 
   while (true) {
-    uint32_t c = 0;  // grab the next group of the schedule
+    uint32_t c = 0;  // grab the next work item of the schedule
     if (lane == 0) c = atomicAdd(&a.work[0], 1u);
     c = __shfl_sync(full, c, 0);
-    if (c >= ngroups) break;
-    const uint32_t gcur = c;
+    if (c >= nitems) break;
+    const uint32_t gcur = c / kStride, part = c % kStride;
     const SegDesc sd = ONE ? a.seg0 : a.L.segs[a.L.seg_of_group[gcur]];
+    if (part >= LPP || (!ONE && sd.wlpp != LPP)) continue;  // another group size's item
     DevState* const sst = a.st + sd.slot;
     const gs_params& P = sst->p;  // read-only during the walk; fields loaded where used
     const float eps2 = __ldg(&P.epsilon2);
@@ -237,8 +266,8 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
     const float qe2 = 0.25f * eps2;
     const bool soft = eps2 > 0.0f;  // self pairs may then be summed and removed afterwards
     const uint32_t seg_end = sd.off + sd.n;
-    const uint32_t gbeg = sd.off + (gcur - sd.group0) * kWalkGroup, gend = gbeg + kWalkGroup;
-    const uint32_t i = gbeg + lane;
+    const uint32_t gbeg = sd.off + (gcur - sd.group0) * kWalkGroup + part * G, gend = gbeg + G;
+    const uint32_t i = gbeg + pl;
     const bool valid = i < seg_end;
     float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0;
     if (valid) {
@@ -250,7 +279,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
     float2 cax = f2(0.f), cay = f2(0.f), caz = f2(0.f), cpt = f2(0.f);  // COMP only
     float dens = 0.f, selfw = 0.f;
     unsigned long long nmono = 0, npair = 0, nvisit = 0;
-    const unsigned all = __ballot_sync(full, valid);
+    const unsigned all = __ballot_sync(full, valid) & GMASK;  // the item's particles (lanes of share 0)
 
     int sp = 0;
     if (lane == 0) S.stack[0] = make_uint2(sd.node_off, all);  // the root: range {node_off, 1}
@@ -323,11 +352,12 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
       uint32_t actbits = 0, keep = 0;  // per range: this lane active; slots this lane may open
 #pragma unroll
       for (int r = 0; r < kWalkRanges; r++) {
-        const uint32_t a_r = (masks[r] >> lane) & 1u;
+        const uint32_t a_r = (masks[r] >> pl) & 1u;
         actbits |= a_r << r;
         const uint32_t cr = (cnts >> (4 * r)) & 15u;
         keep |= a_r ? ((1u << cr) - 1u) << (8 * r) : 0u;
       }
+      keep &= mine;
       // theta^2 per range; a lane inactive for a range tests against -inf, so its
       // td is -inf (or NaN) and it accepts and adds nothing there
       float th2[kWalkRanges];
@@ -335,8 +365,9 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
       for (int r = 0; r < kWalkRanges; r++) th2[r] = (actbits >> r) & 1u ? theta2 : -INFINITY;
       uint32_t obits = 0;  // children this lane opens (active, accept weight 0), bit = slot
 #pragma unroll
-      for (int pp = 0; pp < 4 * kWalkRanges; pp++) {
-        if (pp >= 4 * nr) break;
+      for (int kk = 0; kk < NPP; kk++) {
+        if (kk * LPP >= 4 * nr) break;
+        const int pp = (int)sub + kk * LPP;  // its range (pp >> 2) is (kk * LPP) >> 2 for every share
         const int c = 2 * pp;
         const float2 qx = *reinterpret_cast<const float2*>(&S.cx[c]);
         const float2 qy = *reinterpret_cast<const float2*>(&S.cy[c]);
@@ -345,7 +376,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
         const float2 s2 = *reinterpret_cast<const float2*>(&S.cs2[c]);
         const float2 rx = __fadd2_rn(qx, px), ry = __fadd2_rn(qy, py), rz = __fadd2_rn(qz, pz);
         const float2 d2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __ffma2_rn(rz, rz, f2(eps2))));
-        const float2 td = __fmul2_rn(f2(th2[pp >> 2]), d2);
+        const float2 td = __fmul2_rn(f2(th2[(kk * LPP) >> 2]), d2);
         const float2 w = make_float2(set_gt(td.x, s2.x), set_gt(td.y, s2.y));
         obits |= ((w.x == 0.0f ? 1u : 0u) | (w.y == 0.0f ? 2u : 0u)) << c;
         const float2 rinv = __fmul2_rn(make_float2(rsqrtf(d2.x), rsqrtf(d2.y)), w);
@@ -366,7 +397,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
       obits &= keep;
       const uint32_t om = __reduce_or_sync(full, obits);  // children opened by some lane
       if (DBG) {
-        const uint32_t real = __popc(massmask & keep);
+        const uint32_t real = __popc(massmask & keep);  // keep holds this lane's slots only
         nvisit += real;
         nmono += real - __popc(obits);
       }
@@ -382,8 +413,10 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
       if (!om) continue;
       // Every slot's open mask at once: lane c's col holds the lanes that open
       // slot c (the transpose of the 32 x 32 bit matrix whose rows are the lanes'
-      // obits), so each slot's lane can act on its own child in parallel.
-      const uint32_t col = warp_transpose(obits, lane);
+      // obits), so each slot's lane can act on its own child in parallel. Only
+      // the share that tests slot c has its bits: shifted down, they are the
+      // item's particle mask.
+      const uint32_t col = (warp_transpose(obits, lane) >> ((((uint32_t)lane >> 1) % LPP) * G)) & GMASK;
       // opened internal children: each slot's lane writes its child range and open
       // mask to the stack, in slot order (prefix positions)
       const uint32_t pushc = om & ~leafmask;
@@ -449,8 +482,8 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
           __syncwarp();
           for (uint32_t sl = 0; sl < nb; sl++) {
             const uint4 bl = S.bl[b0 + sl];
-            leaf_sum(S, 16 * sl, bl.y, i - bl.x, (bl.z >> lane) & 1u, soft, px, py, pz, eps2, ax, ay,
-                     az, pt, selfw, npair, DBG);
+            leaf_sum<LPP>(S, 16 * sl, bl.y, i - bl.x, (bl.z >> pl) & 1u, soft, px, py, pz, eps2, ax, ay,
+                          az, pt, selfw, npair, DBG, sub);
           }
         }
       }
@@ -470,8 +503,8 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
           S.lm[lane] = v.w;
           if (lane == 0) S.lx[32] = S.ly[32] = S.lz[32] = S.lm[32] = 0.f;
           __syncwarp();
-          leaf_sum(S, 0, k, i - (cchild + b0), (open >> lane) & 1u, soft, px, py, pz, eps2, ax, ay,
-                   az, pt, selfw, npair, DBG);
+          leaf_sum<LPP>(S, 0, k, i - (cchild + b0), (open >> pl) & 1u, soft, px, py, pz, eps2, ax, ay,
+                        az, pt, selfw, npair, DBG, sub);
         }
       }
     }
@@ -481,10 +514,20 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
       az = __ffma2_rn(caz, f2(-1.0f), az);
       pt = __ffma2_rn(cpt, f2(-1.0f), pt);
     }
+    if (LPP > 1) {  // add the shares of each particle (lanes pl, pl + G, ...), fixed order
+#pragma unroll
+      for (uint32_t o = G; o < 32; o <<= 1) {
+        ax = __fadd2_rn(ax, make_float2(__shfl_xor_sync(full, ax.x, o), __shfl_xor_sync(full, ax.y, o)));
+        ay = __fadd2_rn(ay, make_float2(__shfl_xor_sync(full, ay.x, o), __shfl_xor_sync(full, ay.y, o)));
+        az = __fadd2_rn(az, make_float2(__shfl_xor_sync(full, az.x, o), __shfl_xor_sync(full, az.y, o)));
+        pt = __fadd2_rn(pt, make_float2(__shfl_xor_sync(full, pt.x, o), __shfl_xor_sync(full, pt.y, o)));
+        selfw += __shfl_xor_sync(full, selfw, o);
+      }
+    }
     if (soft && selfw != 0.0f) pt.x -= selfw * p0.w * rsqrtf(eps2);
 
     double e_diag = 0, e_true = 0, mx = 0, my = 0, mz = 0, ms = 0;
-    if (valid) {
+    if (valid && sub == 0) {
       const float G = P.G;
       float fx = (ax.x + ax.y) * G, fy = (ay.x + ay.y) * G, fz = (az.x + az.y) * G;
       const float pot = -(pt.x + pt.y) * G;
@@ -549,11 +592,11 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
       for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(full, v[k], o);
     }
     if (lane < kPartials) {
-      double mine = v[0];
+      double pv = v[0];
 #pragma unroll
       for (int k = 1; k < kPartials; k++)
-        if (lane == k) mine = v[k];
-      a.partials[(size_t)gcur * kPartials + lane] = mine;
+        if (lane == k) pv = v[k];
+      a.partials[((size_t)gcur * kWalkParts + part) * kPartials + lane] = pv;
     }
     if (DBG) {
 #pragma unroll

@@ -113,14 +113,22 @@ int gs_set_star_formation(gs_ctx* ctx, int enable);
  * contributions summed with Kahan compensation. Together with gs_set_com_mode
  * this selects the precision variant; no counterpart in the reference. */
 int gs_set_walk_mode(gs_ctx* ctx, int compensated);
-/* Launch tuning that never changes results (no counterpart in the reference):
+/* Launch tuning (no counterpart in the reference). Takes effect at the next step;
+ * galaxy_sim_b200/autotune.py picks values by timing.
  * GS_TUNE_WALK_BLOCKS_PER_SM = persistent walk blocks per SM (1..8; default 7 for a
  * gs_create context, 8 for a pool; below 8 the walk built for 72 registers per
- * thread runs),
- * GS_TUNE_SORT_ITEMS = keys per thread of a sort tile (8 or 16, default 16). Takes
- * effect at the next step; galaxy_sim_b200/autotune.py picks values by timing. */
+ * thread runs); never changes results.
+ * GS_TUNE_SORT_ITEMS = keys per thread of a sort tile (8 or 16, default 16); never
+ * changes results (a stable sort has one answer).
+ * GS_TUNE_WALK_GROUP = particles a warp walks together: 32 (one lane per particle),
+ * 16 or 8 (two or four lanes per particle, splitting its node tests and leaf
+ * sources), or 0 (default) = by each galaxy's size (8 up to 24576 particles, 16 up
+ * to 98304, else 32). The split changes the order of the force sums, so results
+ * differ at the rounding level (inside the force tolerance) between group sizes;
+ * contexts with the same setting give a galaxy the same result alone or pooled. */
 #define GS_TUNE_WALK_BLOCKS_PER_SM 1
 #define GS_TUNE_SORT_ITEMS 2
+#define GS_TUNE_WALK_GROUP 3
 int gs_set_tuning(gs_ctx* ctx, int knob, int value);
 int gs_get_tuning(gs_ctx* ctx, int knob, int* value);
 /* NBodyGPU.updateCentralMass (NBodyGPU.js:245-251): both ping-pong buffers. */
