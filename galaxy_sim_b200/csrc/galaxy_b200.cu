@@ -235,7 +235,7 @@ struct gs_ctx {
   int com_mode = kComF32;
   int sort_items = kSortItems;     // tuning: keys per thread of a sort tile (8 or 16)
   int walk_bps = kWalkBlocksPerSM; // tuning: persistent walk blocks per SM (1..8; < 8: 72-register build)
-  int walk_group = 0;              // tuning: walk group size (0: by galaxy size; 8, 16 or 32 particles)
+  int walk_group = 32;             // tuning: walk group size (0: by galaxy size; 8, 16 or 32 particles)
   uint32_t walk_items[3] = {0, 0, 0};  // work items of the layout per lanes-per-particle class (1, 2, 4)
   bool walk_comp = false;  // Kahan-compensated far-field sums in the walk
   void* host_stage = nullptr;  // pinned: [slots] params
@@ -957,6 +957,7 @@ int gs_create_on(int device, uint32_t N, const float* particles8, const float* s
   c->palloc.init(0);
   c->single = true;
   c->walk_bps = kWalkBlocksWide;  // one galaxy: the 72-register walk measured faster
+  c->walk_group = 0;              // one galaxy: walk groups by its size (a pool fills the GPU with 32s)
   return GS_OK;
 }
 

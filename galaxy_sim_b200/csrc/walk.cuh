@@ -55,10 +55,11 @@ constexpr int kWalkBlocksPerSM = 8;
 constexpr int kWalkBlocksWide = 7;
 constexpr uint32_t kWalkGroup = 32;             // particles per walk group (layout, diagnostics)
 constexpr uint32_t kWalkParts = 4;              // work items per group in a pool (the largest LPP)
-// galaxies of at most this many particles walk in groups of 8 / 16 particles
-// (the context's default; GS_TUNE_WALK_GROUP forces one size)
-constexpr uint32_t kWalkAuto8 = 24576;
-constexpr uint32_t kWalkAuto16 = 98304;
+// with the walk group chosen by size, galaxies of at most this many particles
+// walk in groups of 8 / 16 particles (measured crossovers of the step time on a
+// B200: 8 is fastest up to 32768 particles, 16 at 65536, 32 from 262144 on)
+constexpr uint32_t kWalkAuto8 = 45000;
+constexpr uint32_t kWalkAuto16 = 150000;
 
 // nbody_bh.wgsl:206-213
 __device__ inline uint32_t pcg(uint32_t v0) {
@@ -134,11 +135,16 @@ struct WalkArgs {
 // Per-warp shared staging.
 struct WalkSmem {
   uint2 stack[kWalkStack];          // {first child | (count-1) << 29, lane mask}
-  float cx[8 * kWalkRanges], cy[8 * kWalkRanges], cz[8 * kWalkRanges];  // staged child ranges
-  float cmass[8 * kWalkRanges], cs2[8 * kWalkRanges];
+  // staged child ranges, pair-interleaved so a packed test reads two 128-bit
+  // words: cxy[4p..4p+3] = {x(2p), x(2p+1), y(2p), y(2p+1)}, czm likewise {z, m}
+  __align__(16) float cxy[16 * kWalkRanges];
+  __align__(16) float czm[16 * kWalkRanges];
+  float cs2[8 * kWalkRanges];
   uint32_t cnode[8 * kWalkRanges];  // node index of each staged child
   uint4 cmeta[8 * kWalkRanges];     // {child, info, own-leaf size bits, massive}
-  float lx[66], ly[66], lz[66], lm[66];
+  // staged leaf sources, pair-interleaved the same way (pairs 0..32)
+  __align__(16) float lxy[136];
+  __align__(16) float lzm[136];
   uint4 bl[8 * kWalkRanges];        // opened small leaves: {first particle, count, lane mask, 0}
 };
 
@@ -158,10 +164,10 @@ __device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k
     const float2 wme = make_float2(me ? 1.0f : 0.0f, me ? 1.0f : 0.0f);
     if (me && jself < k && ((jself >> 1) % LPP) == sub) selfw += 1.0f;
     for (uint32_t j = 2 * sub; j < k; j += 2 * LPP) {
-      const float2 jx = *reinterpret_cast<const float2*>(&S.lx[off + j]);
-      const float2 jy = *reinterpret_cast<const float2*>(&S.ly[off + j]);
-      const float2 jz = *reinterpret_cast<const float2*>(&S.lz[off + j]);
-      const float2 jm = *reinterpret_cast<const float2*>(&S.lm[off + j]);
+      const float4 jxy = *reinterpret_cast<const float4*>(&S.lxy[2 * (off + j)]);
+      const float4 jzm = *reinterpret_cast<const float4*>(&S.lzm[2 * (off + j)]);
+      const float2 jx = make_float2(jxy.x, jxy.y), jy = make_float2(jxy.z, jxy.w);
+      const float2 jz = make_float2(jzm.x, jzm.y), jm = make_float2(jzm.z, jzm.w);
       const float2 ex = __fadd2_rn(jx, px), ey = __fadd2_rn(jy, py), ez = __fadd2_rn(jz, pz);
       const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __ffma2_rn(ez, ez, make_float2(eps2, eps2))));
       const float2 ri = __fmul2_rn(make_float2(rsqrtf(e2.x), rsqrtf(e2.y)), wme);
@@ -175,10 +181,10 @@ __device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k
     }
   } else {
     for (uint32_t j = 2 * sub; j < k; j += 2 * LPP) {
-      const float2 jx = *reinterpret_cast<const float2*>(&S.lx[off + j]);
-      const float2 jy = *reinterpret_cast<const float2*>(&S.ly[off + j]);
-      const float2 jz = *reinterpret_cast<const float2*>(&S.lz[off + j]);
-      const float2 jm = *reinterpret_cast<const float2*>(&S.lm[off + j]);
+      const float4 jxy = *reinterpret_cast<const float4*>(&S.lxy[2 * (off + j)]);
+      const float4 jzm = *reinterpret_cast<const float4*>(&S.lzm[2 * (off + j)]);
+      const float2 jx = make_float2(jxy.x, jxy.y), jy = make_float2(jxy.z, jxy.w);
+      const float2 jz = make_float2(jzm.x, jzm.y), jm = make_float2(jzm.z, jzm.w);
       const float2 ex = __fadd2_rn(jx, px), ey = __fadd2_rn(jy, py), ez = __fadd2_rn(jz, pz);
       const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __ffma2_rn(ez, ez, make_float2(eps2, eps2))));
       const bool u0 = me && j != jself;
@@ -335,10 +341,11 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
         } else if (s2 < qe2) {
           s2 = -INFINITY;
         }
-        S.cx[lane] = q.x;
-        S.cy[lane] = q.y;
-        S.cz[lane] = q.z;
-        S.cmass[lane] = q.w;
+        const int st = 4 * (lane >> 1) + (lane & 1);
+        S.cxy[st] = q.x;
+        S.cxy[st + 2] = q.y;
+        S.czm[st] = q.z;
+        S.czm[st + 2] = q.w;
         S.cs2[lane] = s2;
         S.cnode[lane] = rs + c;
         S.cmeta[lane] = make_uint4(w.child, w.info,
@@ -369,10 +376,10 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
         if (kk * LPP >= 4 * nr) break;
         const int pp = (int)sub + kk * LPP;  // its range (pp >> 2) is (kk * LPP) >> 2 for every share
         const int c = 2 * pp;
-        const float2 qx = *reinterpret_cast<const float2*>(&S.cx[c]);
-        const float2 qy = *reinterpret_cast<const float2*>(&S.cy[c]);
-        const float2 qz = *reinterpret_cast<const float2*>(&S.cz[c]);
-        const float2 qm = *reinterpret_cast<const float2*>(&S.cmass[c]);
+        const float4 qxy = *reinterpret_cast<const float4*>(&S.cxy[2 * c]);
+        const float4 qzm = *reinterpret_cast<const float4*>(&S.czm[2 * c]);
+        const float2 qx = make_float2(qxy.x, qxy.y), qy = make_float2(qxy.z, qxy.w);
+        const float2 qz = make_float2(qzm.x, qzm.y), qm = make_float2(qzm.z, qzm.w);
         const float2 s2 = *reinterpret_cast<const float2*>(&S.cs2[c]);
         const float2 rx = __fadd2_rn(qx, px), ry = __fadd2_rn(qy, py), rz = __fadd2_rn(qz, pz);
         const float2 d2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __ffma2_rn(rz, rz, f2(eps2))));
@@ -473,10 +480,11 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
               const uint4 bl = S.bl[b0 + slot];
               float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
               if (q < bl.y) v = __ldg(&a.pin[2 * (size_t)(bl.x + q)]);
-              S.lx[e] = v.x;
-              S.ly[e] = v.y;
-              S.lz[e] = v.z;
-              S.lm[e] = v.w;
+              const uint32_t se = 4 * (e >> 1) + (e & 1);
+              S.lxy[se] = v.x;
+              S.lxy[se + 2] = v.y;
+              S.lzm[se] = v.z;
+              S.lzm[se + 2] = v.w;
             }
           }
           __syncwarp();
@@ -497,11 +505,12 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
           __syncwarp();
           float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
           if (lane < (int)k) v = __ldg(&a.pin[2 * (size_t)(cchild + b0 + lane)]);
-          S.lx[lane] = v.x;
-          S.ly[lane] = v.y;
-          S.lz[lane] = v.z;
-          S.lm[lane] = v.w;
-          if (lane == 0) S.lx[32] = S.ly[32] = S.lz[32] = S.lm[32] = 0.f;
+          const int se = 4 * (lane >> 1) + (lane & 1);
+          S.lxy[se] = v.x;
+          S.lxy[se + 2] = v.y;
+          S.lzm[se] = v.z;
+          S.lzm[se + 2] = v.w;
+          if (lane == 0) S.lxy[64] = S.lxy[66] = S.lzm[64] = S.lzm[66] = 0.f;  // source 32
           __syncwarp();
           leaf_sum<LPP>(S, 0, k, i - (cchild + b0), (open >> pl) & 1u, soft, px, py, pz, eps2, ax, ay,
                         az, pt, selfw, npair, DBG, sub);

@@ -41,7 +41,9 @@ def build_params(N, *, dt, G, epsilon, theta=0.5, haloMass=0, haloA=1, gasDrag=0
 
 
 class NBodyGPU:
-    def __init__(self, device, particleData, stellarData=None):
+    def __init__(self, device, particleData, stellarData=None, walkGroup=None):
+        """walkGroup: particles a warp walks together (8, 16, 32, or 0 = by size,
+        the default of a single-galaxy context; a pool uses 32)."""
         P = f32(particleData).ravel()
         if P.size % 8:
             raise ValueError("particleData must hold 8 floats per particle")
@@ -56,6 +58,10 @@ class NBodyGPU:
         self.ready = True
         self.levelRanges = None
         self._params = GsParams()
+        if walkGroup is not None:
+            from ._lib import TUNE_WALK_GROUP
+
+            self._ok(lib().gs_set_tuning(self._ctx, TUNE_WALK_GROUP, int(walkGroup)))
 
     # -- reference surface --------------------------------------------------------------
     def _ok(self, rc):

@@ -122,10 +122,13 @@ int gs_set_walk_mode(gs_ctx* ctx, int compensated);
  * changes results (a stable sort has one answer).
  * GS_TUNE_WALK_GROUP = particles a warp walks together: 32 (one lane per particle),
  * 16 or 8 (two or four lanes per particle, splitting its node tests and leaf
- * sources), or 0 (default) = by each galaxy's size (8 up to 24576 particles, 16 up
- * to 98304, else 32). The split changes the order of the force sums, so results
- * differ at the rounding level (inside the force tolerance) between group sizes;
- * contexts with the same setting give a galaxy the same result alone or pooled. */
+ * sources), or 0 = by each galaxy's size (8 up to 45000 particles, 16 up to
+ * 150000, else 32). Default: 0 for a gs_create context (a small galaxy alone needs
+ * the smaller groups to fill the GPU), 32 for a pool (many galaxies fill it; 32
+ * costs the fewest instructions). The split changes the order of the force sums,
+ * so results differ at the rounding level (inside the force tolerance) between
+ * group sizes; with the same setting a galaxy gets the same result alone or
+ * pooled. */
 #define GS_TUNE_WALK_BLOCKS_PER_SM 1
 #define GS_TUNE_SORT_ITEMS 2
 #define GS_TUNE_WALK_GROUP 3

@@ -39,8 +39,8 @@ def _tracking(g):
     return (c1, c2, hc[0] if len(hc) > 0 else None, hc[1] if len(hc) > 1 else None)
 
 
-def _solo(g, ph, steps, sf):
-    sim = NBodyGPU(0, g.particles, g.stellar)
+def _solo(g, ph, steps, sf, walk_group=32):
+    sim = NBodyGPU(0, g.particles, g.stellar, walkGroup=walk_group)  # the pool's setting
     sim.updateParams(**params_dict(g, ph))
     t = _tracking(g)
     if t is not None:
@@ -81,6 +81,26 @@ def test_batch_equals_solo_runs(gpu_lib):
     E = pool.energies()
     for s, solo in zip(slots, solos):
         assert E[s, 0] == solo[2]["e_diag"]
+    pool.close()
+
+
+def test_batch_equals_solo_with_walk_groups_by_size(gpu_lib):
+    """With the walk group chosen by each galaxy's size (8, 16 or 32 particles
+    per warp, one walk launch per size class in the pool), every galaxy still
+    equals its solo run with the same setting, bit for bit."""
+    from galaxy_sim_b200 import _lib
+
+    cases = _cases() + [(ic.galaxy_disk(90000, 16, gas_frac=0.3), Physics(0.02, 0.5, 0.005, gas_drag=0.25,
+                                                                        sf_eff=0.02)),
+                        (ic.galaxy_disk(160000, 17), Physics(0.02, 0.7, 0.005))]
+    steps = 2
+    solos = [_solo(g, ph, steps, True, walk_group=0) for g, ph in cases]
+    pool = GalaxyPool(sum(g.N + 256 for g, _ in cases) + 4096, 8)
+    _lib.check(_lib.lib().gs_set_tuning(pool._ctx, _lib.TUNE_WALK_GROUP, 0), pool._ctx)
+    slots = [pool.add(g.particles, g.stellar, params_dict(g, ph), _tracking(g)) for g, ph in cases]
+    pool.run(steps, True)
+    for s, solo in zip(slots, solos):
+        _check_same(pool, s, solo)
     pool.close()
 
 
@@ -150,7 +170,7 @@ def test_batch_equals_solo_in_precision_modes(gpu_lib, comp, com64):
     steps = 2
     solos = []
     for g, ph in cases:
-        sim = NBodyGPU(0, g.particles, g.stellar)
+        sim = NBodyGPU(0, g.particles, g.stellar, walkGroup=32)   # the pool's walk group
         sim.updateParams(**params_dict(g, ph))
         t = _tracking(g)
         if t is not None:

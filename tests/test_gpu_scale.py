@@ -2,7 +2,8 @@
 
 * The batched ensemble: the seeded 96-galaxy set (N log-uniform in [4096,
   262144], 4.65 M particles, gas with drag and star formation in about half of
-  them) stepped as one pool. Every galaxy equals its solo run bit for bit. For
+  them) stepped as one pool. Every galaxy equals its solo run (same walk group
+  size) bit for bit. For
   eight galaxies, the largest included, the pool's own rebuild equals the
   oracle's sortAndBuild (permutation and topology bit-exact) and the pool's
   forces fall within the tolerance of the FP64 walk of the same acceptance rule
@@ -10,7 +11,7 @@
 * The served stream: requests drawn from the served ranges (a disk of 2^20, the
   collision and sphere presets, eps/theta/dt from their sets) pushed through a
   continuous-batching server too small to hold them at once. Every result
-  equals the same request run alone, bit for bit.
+  equals the same request run alone (same walk group size), bit for bit.
 * The long run: 1000 steps of the disk of N = 524288 with gas drag and star
   formation. The device's energy drift follows the oracle's FP32 run of the
   reference scheme on the same initial conditions (a committed trajectory,
@@ -57,7 +58,7 @@ def test_batch96_pool_equals_solo_and_forces_within_tolerance(gpu_lib, oracle):
     assert None not in slots
     pool.run(steps, True)
     for (g, ph), s in zip(gals, slots):
-        solo = NBodyGPU(0, g.particles, g.stellar)
+        solo = NBodyGPU(0, g.particles, g.stellar, walkGroup=32)   # the pool's walk group
         solo.updateParams(**params_dict(g, ph))
         solo.run(steps, ph.sf_eff > 0)
         SP, SS = solo.readState()
@@ -128,7 +129,7 @@ def test_served_stream_at_request_scale_equals_alone(gpu_lib):
     assert stats["particle_steps"] == sum(r.N * r.steps for r in reqs)
     assert max(r.admitted - r.arrival for r in reqs) > 0     # the pool could not hold them all
     for r in reqs:
-        sim = NBodyGPU(0, r.particles, r.stellar)
+        sim = NBodyGPU(0, r.particles, r.stellar, walkGroup=32)   # the pool's walk group
         sim.updateParams(**r.params)
         if r.tracking is not None:
             sim.setTracking(*r.tracking)
