@@ -3,8 +3,8 @@
 Knobs (`gs_set_tuning`):
 
 * walk group size: how many particles a warp walks together, 32 (one lane per
-  particle), 16 or 8 (two or four lanes per particle splitting its node tests
-  and leaf sources), or 0 = by each galaxy's size. Small galaxies need the
+  particle), 16, 8 or 4 (two, four or eight lanes per particle splitting its
+  node tests and leaf sources), or 0 = by each galaxy's size. Small galaxies need the
   smaller groups to fill the GPU; large ones walk fastest in groups of 32. The
   group size changes the order of the force sums, so results change at the
   rounding level (inside the force tolerance) with it;
@@ -32,7 +32,7 @@ from ._lib import TUNE_SORT_ITEMS, TUNE_WALK_BLOCKS_PER_SM, TUNE_WALK_GROUP, Gal
 
 WALK_BLOCKS = (6, 7, 8)
 SORT_ITEMS = (8, 16)
-WALK_GROUPS = (0, 8, 16, 32)
+WALK_GROUPS = (0, 4, 8, 16, 32)
 
 
 def get(ctx, knob: int) -> int:

@@ -235,8 +235,8 @@ struct gs_ctx {
   int com_mode = kComF32;
   int sort_items = kSortItems;     // tuning: keys per thread of a sort tile (8 or 16)
   int walk_bps = kWalkBlocksPerSM; // tuning: persistent walk blocks per SM (1..8; < 8: 72-register build)
-  int walk_group = 32;             // tuning: walk group size (0: by galaxy size; 8, 16 or 32 particles)
-  uint32_t walk_items[3] = {0, 0, 0};  // work items of the layout per lanes-per-particle class (1, 2, 4)
+  int walk_group = 32;             // tuning: walk group size (0: by galaxy size; 4, 8, 16 or 32 particles)
+  uint32_t walk_items[4] = {0, 0, 0, 0};  // work items per lanes-per-particle class (1, 2, 4, 8)
   bool walk_comp = false;  // Kahan-compensated far-field sums in the walk
   void* host_stage = nullptr;  // pinned: [slots] params
   std::map<int, cudaGraphExec_t> graphs;
@@ -403,9 +403,11 @@ void pool_release(gs_ctx* c) {
 // size, or by size (a small galaxy walks in groups of 8 or 16 particles so that
 // its walk fills more warps).
 uint32_t walk_lpp(const gs_ctx* c, uint32_t n) {
+  if (c->walk_group == 4) return 8;
   if (c->walk_group == 8) return 4;
   if (c->walk_group == 16) return 2;
   if (c->walk_group == 32) return 1;
+  if (n <= kWalkAuto4) return 8;
   if (n <= kWalkAuto8) return 4;
   if (n <= kWalkAuto16) return 2;
   return 1;
@@ -422,7 +424,7 @@ int ensure_layout(gs_ctx* c) {
             [&](uint32_t a, uint32_t b) { return c->slots[a].off < c->slots[b].off; });
   std::vector<SegDesc> h(order.size());
   uint32_t st = 0, ft = 0, gr = 0, dc = 0, hs = 0;
-  uint32_t items[3] = {0, 0, 0};
+  uint32_t items[4] = {0, 0, 0, 0};
   for (size_t r = 0; r < order.size(); r++) {
     Slot& s = c->slots[order[r]];
     s.rank = (uint32_t)r;
@@ -443,7 +445,7 @@ int ensure_layout(gs_ctx* c) {
     dc += cdiv(cdiv(s.n, kWalkGroup), kDiagChunk);
     st += cdiv(s.n, (uint64_t)kSortThreads * c->sort_items);
     ft += cdiv(s.n, kFlagTile);
-    items[h[r].wlpp == 1 ? 0 : h[r].wlpp == 2 ? 1 : 2] += cdiv(s.n, kWalkGroup) * h[r].wlpp;
+    items[h[r].wlpp == 1 ? 0 : h[r].wlpp == 2 ? 1 : h[r].wlpp == 4 ? 2 : 3] += cdiv(s.n, kWalkGroup) * h[r].wlpp;
     gr += cdiv(s.n, kWalkGroup);
     hs = std::max(hs, order[r] + 1);
   }
@@ -470,9 +472,9 @@ int ensure_layout(gs_ctx* c) {
   L.diag_chunks = dc;
   c->hist_slots = hs;
   c->seg_host = h;
-  const uint32_t most = std::max(items[0], std::max(items[1], items[2]));
+  const uint32_t most = std::max(std::max(items[0], items[1]), std::max(items[2], items[3]));
   c->walk_grid = std::min<uint32_t>(std::max<uint32_t>(1, cdiv(most, kWalkWarps)), (uint32_t)c->sms * c->walk_bps);
-  for (int k = 0; k < 3; k++) c->walk_items[k] = items[k];
+  for (int k = 0; k < 4; k++) c->walk_items[k] = items[k];
   c->drop_graphs();
   c->lay_dirty = false;
   return GS_OK;
@@ -591,11 +593,12 @@ void enqueue_walk(gs_ctx* c, int sf) {
   const int v = (sf ? 1 : 0) | (c->debug ? 2 : 0) | (one ? 4 : 0) | (c->walk_comp ? 8 : 0);
   // one launch per walk group size present (a single galaxy: its own); 8 blocks
   // per SM: the 64-register build, fewer: the 72-register build (groups of 32)
-  for (int k = 0; k < 3; k++) {
+  for (int k = 0; k < 4; k++) {
     if (!c->walk_items[k]) continue;
     const uint32_t gk = std::min<uint32_t>(g, std::max<uint32_t>(1, cdiv(c->walk_items[k], kWalkWarps)));
     if (k == 1) launch_walk<kWalkBlocksPerSM, 2>(v, gk, s, a);
     else if (k == 2) launch_walk<kWalkBlocksPerSM, 4>(v, gk, s, a);
+    else if (k == 3) launch_walk<kWalkBlocksPerSM, 8>(v, gk, s, a);
     else if (c->walk_bps >= kWalkBlocksPerSM) launch_walk<kWalkBlocksPerSM, 1>(v, gk, s, a);
     else launch_walk<kWalkBlocksWide, 1>(v, gk, s, a);
   }
@@ -1226,8 +1229,8 @@ int gs_set_tuning(gs_ctx* ctx, int knob, int value) {
     if (value != 8 && value != 16) return ctx->fail(GS_EINVAL, "sort keys per thread must be 8 or 16");
     ctx->sort_items = value;
   } else if (knob == GS_TUNE_WALK_GROUP) {
-    if (value != 0 && value != 8 && value != 16 && value != 32)
-      return ctx->fail(GS_EINVAL, "walk group must be 0 (by galaxy size), 8, 16 or 32 particles");
+    if (value != 0 && value != 4 && value != 8 && value != 16 && value != 32)
+      return ctx->fail(GS_EINVAL, "walk group must be 0 (by galaxy size), 4, 8, 16 or 32 particles");
     ctx->walk_group = value;
   } else {
     return ctx->fail(GS_EINVAL, "unknown tuning knob %d", knob);

@@ -22,8 +22,8 @@
 //   * Warps are persistent and take work items from an atomic counter (load
 //     balance across the dense core); per-item FP64 partials of the
 //     diagnostics replace a block-wide barrier.
-//   * Walk group size: a work item is 32, 16 or 8 Morton-consecutive particles
-//     (LPP = 1, 2 or 4 lanes per particle). With LPP > 1 the lanes of a
+//   * Walk group size: a work item is 32, 16, 8 or 4 Morton-consecutive
+//     particles (LPP = 1, 2, 4 or 8 lanes per particle). With LPP > 1 the lanes of a
 //     particle split the round's slot pairs and each opened leaf's source pairs
 //     between them and add their partial sums by shuffles at the end, so a
 //     small galaxy keeps more warps busy and each warp walks the union of
@@ -54,10 +54,12 @@ constexpr int kWalkStack = 8 * 11 * kWalkRanges;
 constexpr int kWalkBlocksPerSM = 8;
 constexpr int kWalkBlocksWide = 7;
 constexpr uint32_t kWalkGroup = 32;             // particles per walk group (layout, diagnostics)
-constexpr uint32_t kWalkParts = 4;              // work items per group in a pool (the largest LPP)
+constexpr uint32_t kWalkParts = 8;              // partial-sum slots per walk group (the largest LPP)
 // with the walk group chosen by size, galaxies of at most this many particles
-// walk in groups of 8 / 16 particles (measured crossovers of the step time on a
-// B200: 8 is fastest up to 32768 particles, 16 at 65536, 32 from 262144 on)
+// walk in groups of 4 / 8 / 16 particles (measured crossovers of the step time
+// on a B200: 4 is fastest at 4096-8192 particles, 8 up to 32768, 16 at 65536,
+// 32 from 262144 on)
+constexpr uint32_t kWalkAuto4 = 12000;
 constexpr uint32_t kWalkAuto8 = 45000;
 constexpr uint32_t kWalkAuto16 = 150000;
 
@@ -149,13 +151,15 @@ struct WalkSmem {
 };
 
 // Direct sum of a staged leaf segment [off, off + k) for the lanes in `me`
-// (nbody_bh.wgsl:117-131), two sources per packed step. A particle served by
-// LPP lanes splits the source pairs: lane `sub` takes pairs sub, sub + LPP, ...
-// With soft (eps^2 > 0) the self pair is included (zero force at r = 0) and its
-// potential removed once at the end of the walk via selfw (counted by the lane
-// whose share holds it); otherwise it is skipped per pair.
+// (nbody_bh.wgsl:117-131), two sources per packed step, up to kmax >= k (staged
+// sources past a leaf's count are massless zeros). A particle served by LPP
+// lanes splits the source pairs: lane
+// `sub` takes pairs sub, sub + LPP, ... With soft (eps^2 > 0) the self pair is
+// included (zero force at r = 0) and its potential removed once at the end of
+// the walk via selfw (counted by the lane whose share holds it); otherwise it is
+// skipped per pair.
 template <int LPP, typename Smem>
-__device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k, uint32_t jself,
+__device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k, uint32_t kmax, uint32_t jself,
                                          bool me, bool soft, float2 px, float2 py, float2 pz,
                                          float eps2, float2& ax, float2& ay, float2& az,
                                          float2& pt, float& selfw, unsigned long long& npair,
@@ -163,7 +167,7 @@ __device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k
   if (soft) {
     const float2 wme = make_float2(me ? 1.0f : 0.0f, me ? 1.0f : 0.0f);
     if (me && jself < k && ((jself >> 1) % LPP) == sub) selfw += 1.0f;
-    for (uint32_t j = 2 * sub; j < k; j += 2 * LPP) {
+    for (uint32_t j = 2 * sub; j < kmax; j += 2 * LPP) {
       const float4 jxy = *reinterpret_cast<const float4*>(&S.lxy[2 * (off + j)]);
       const float4 jzm = *reinterpret_cast<const float4*>(&S.lzm[2 * (off + j)]);
       const float2 jx = make_float2(jxy.x, jxy.y), jy = make_float2(jxy.z, jxy.w);
@@ -177,17 +181,17 @@ __device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k
       ay = __ffma2_rn(ey, ff, ay);
       az = __ffma2_rn(ez, ff, az);
       pt = __fadd2_rn(pt, mr);
-      if (dbg && me) npair += (j != jself) + (j + 1 < k && j + 1 != jself);
+      if (dbg && me) npair += (j < k && j != jself) + (j + 1 < k && j + 1 != jself);
     }
   } else {
-    for (uint32_t j = 2 * sub; j < k; j += 2 * LPP) {
+    for (uint32_t j = 2 * sub; j < kmax; j += 2 * LPP) {
       const float4 jxy = *reinterpret_cast<const float4*>(&S.lxy[2 * (off + j)]);
       const float4 jzm = *reinterpret_cast<const float4*>(&S.lzm[2 * (off + j)]);
       const float2 jx = make_float2(jxy.x, jxy.y), jy = make_float2(jxy.z, jxy.w);
       const float2 jz = make_float2(jzm.x, jzm.y), jm = make_float2(jzm.z, jzm.w);
       const float2 ex = __fadd2_rn(jx, px), ey = __fadd2_rn(jy, py), ez = __fadd2_rn(jz, pz);
       const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __ffma2_rn(ez, ez, make_float2(eps2, eps2))));
-      const bool u0 = me && j != jself;
+      const bool u0 = me && j < k && j != jself;
       const bool u1 = me && j + 1 < k && j + 1 != jself;
       const float2 ri = make_float2(u0 ? rsqrtf(e2.x) : 0.0f, u1 ? rsqrtf(e2.y) : 0.0f);
       const float2 mr = __fmul2_rn(jm, ri);
@@ -241,18 +245,21 @@ __device__ __forceinline__ uint32_t warp_transpose(uint32_t x, int lane) {
 // galaxies whose SegDesc wlpp field equals LPP and skips the others' work items.
 template <bool SF, bool DBG, bool ONE, bool COMP, int MINB, int LPP>
 __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
-  static_assert(LPP == 1 || LPP == 2 || LPP == 4, "lanes per particle");
+  static_assert(LPP == 1 || LPP == 2 || LPP == 4 || LPP == 8, "lanes per particle");
   constexpr uint32_t G = 32 / LPP;                         // particles per work item
   constexpr int NPP = 16 / LPP;                            // slot pairs a lane tests in a full round
   constexpr unsigned GMASK = G == 32 ? 0xffffffffu : (1u << G) - 1u;
-  constexpr uint32_t kStride = ONE ? LPP : kWalkParts;    // work items per walk group
+  constexpr uint32_t kStride = LPP;                        // work items per walk group
   griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
   __shared__ WalkSmem smem_all[kWalkWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t pl = lane % G;    // the lane's particle within the item
   const uint32_t sub = lane / G;   // its share of the slot pairs and leaf sources
   // slots whose pairs this lane tests: pairs sub, sub + LPP, ... (bits 2pp, 2pp + 1)
-  const uint32_t mine = LPP == 1 ? 0xffffffffu : LPP == 2 ? (0x33333333u << (2 * sub)) : (0x03030303u << (2 * sub));
+  const uint32_t mine = LPP == 1   ? 0xffffffffu
+                        : LPP == 2 ? (0x33333333u << (2 * sub))
+                        : LPP == 4 ? (0x03030303u << (2 * sub))
+                                   : (0x00030003u << (2 * sub));
   WalkSmem& S = smem_all[warp];
   const uint32_t nitems = a.L.groups * kStride;
   const unsigned full = 0xffffffffu;
@@ -264,7 +271,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
     if (c >= nitems) break;
     const uint32_t gcur = c / kStride, part = c % kStride;
     const SegDesc sd = ONE ? a.seg0 : a.L.segs[a.L.seg_of_group[gcur]];
-    if (part >= LPP || (!ONE && sd.wlpp != LPP)) continue;  // another group size's item
+    if (!ONE && sd.wlpp != LPP) continue;  // a galaxy of another group size
     DevState* const sst = a.st + sd.slot;
     const gs_params& P = sst->p;  // read-only during the walk; fields loaded where used
     const float eps2 = __ldg(&P.epsilon2);
@@ -374,8 +381,10 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
 #pragma unroll
       for (int kk = 0; kk < NPP; kk++) {
         if (kk * LPP >= 4 * nr) break;
-        const int pp = (int)sub + kk * LPP;  // its range (pp >> 2) is (kk * LPP) >> 2 for every share
+        const int pp = (int)sub + kk * LPP;
         const int c = 2 * pp;
+        // the pair's range pp >> 2: (kk * LPP) >> 2 for shares below 4, one more above
+        const float t2 = LPP < 8 ? th2[(kk * LPP) >> 2] : (sub >= 4 ? th2[2 * kk + 1] : th2[2 * kk]);
         const float4 qxy = *reinterpret_cast<const float4*>(&S.cxy[2 * c]);
         const float4 qzm = *reinterpret_cast<const float4*>(&S.czm[2 * c]);
         const float2 qx = make_float2(qxy.x, qxy.y), qy = make_float2(qxy.z, qxy.w);
@@ -383,7 +392,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
         const float2 s2 = *reinterpret_cast<const float2*>(&S.cs2[c]);
         const float2 rx = __fadd2_rn(qx, px), ry = __fadd2_rn(qy, py), rz = __fadd2_rn(qz, pz);
         const float2 d2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __ffma2_rn(rz, rz, f2(eps2))));
-        const float2 td = __fmul2_rn(f2(th2[(kk * LPP) >> 2]), d2);
+        const float2 td = __fmul2_rn(f2(t2), d2);
         const float2 w = make_float2(set_gt(td.x, s2.x), set_gt(td.y, s2.y));
         obits |= ((w.x == 0.0f ? 1u : 0u) | (w.y == 0.0f ? 2u : 0u)) << c;
         const float2 rinv = __fmul2_rn(make_float2(rsqrtf(d2.x), rsqrtf(d2.y)), w);
@@ -490,7 +499,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
           __syncwarp();
           for (uint32_t sl = 0; sl < nb; sl++) {
             const uint4 bl = S.bl[b0 + sl];
-            leaf_sum<LPP>(S, 16 * sl, bl.y, i - bl.x, (bl.z >> pl) & 1u, soft, px, py, pz, eps2, ax, ay,
+            leaf_sum<LPP>(S, 16 * sl, bl.y, bl.y, i - bl.x, (bl.z >> pl) & 1u, soft, px, py, pz, eps2, ax, ay,
                           az, pt, selfw, npair, DBG, sub);
           }
         }
@@ -512,7 +521,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
           S.lzm[se + 2] = v.w;
           if (lane == 0) S.lxy[64] = S.lxy[66] = S.lzm[64] = S.lzm[66] = 0.f;  // source 32
           __syncwarp();
-          leaf_sum<LPP>(S, 0, k, i - (cchild + b0), (open >> pl) & 1u, soft, px, py, pz, eps2, ax, ay,
+          leaf_sum<LPP>(S, 0, k, k, i - (cchild + b0), (open >> pl) & 1u, soft, px, py, pz, eps2, ax, ay,
                         az, pt, selfw, npair, DBG, sub);
         }
       }

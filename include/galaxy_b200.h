@@ -121,9 +121,9 @@ int gs_set_walk_mode(gs_ctx* ctx, int compensated);
  * GS_TUNE_SORT_ITEMS = keys per thread of a sort tile (8 or 16, default 16); never
  * changes results (a stable sort has one answer).
  * GS_TUNE_WALK_GROUP = particles a warp walks together: 32 (one lane per particle),
- * 16 or 8 (two or four lanes per particle, splitting its node tests and leaf
- * sources), or 0 = by each galaxy's size (8 up to 45000 particles, 16 up to
- * 150000, else 32). Default: 0 for a gs_create context (a small galaxy alone needs
+ * 16, 8 or 4 (two, four or eight lanes per particle, splitting its node tests and
+ * leaf sources), or 0 = by each galaxy's size (4 up to 12000 particles, 8 up to
+ * 45000, 16 up to 150000, else 32). Default: 0 for a gs_create context (a small galaxy alone needs
  * the smaller groups to fill the GPU), 32 for a pool (many galaxies fill it; 32
  * costs the fewest instructions). The split changes the order of the force sums,
  * so results differ at the rounding level (inside the force tolerance) between

@@ -61,7 +61,7 @@ def _rel(a, b):
 def test_walk_group_sizes_agree(gpu_lib, oracle, n, eps):
     g = ic.galaxy_disk(n, 9, Q=1.2, arms=4, gas_frac=0.3)
     out = {}
-    for wg in (32, 16, 8, 0):
+    for wg in (32, 16, 8, 4, 0):
         sim = NBodyGPU(0, g.particles, g.stellar)
         sim.updateParams(dt=0.005, G=1.0, epsilon=eps, theta=0.5)
         set_(sim._ctx, _lib.TUNE_WALK_GROUP, wg)
@@ -98,7 +98,7 @@ def test_autotune_pool(gpu_lib):
         pool.add(g.particles, g.stellar, params_dict(g, Physics(0.05, 0.5, 0.005)))
     res = autotune(pool, steps=2, warmup=1, walk_blocks=(4, 8), sort_items=(8, 16))
     ch = res["choice"]
-    assert len(res["ms"]) == 8 and all(t > 0 for t in res["ms"].values())
+    assert len(res["ms"]) == 9 and all(t > 0 for t in res["ms"].values())
     assert get(pool._ctx, _lib.TUNE_WALK_GROUP) == (0 if ch["walk_group"] == "by galaxy size" else ch["walk_group"])
     assert get(pool._ctx, _lib.TUNE_WALK_BLOCKS_PER_SM) == ch["walk_blocks_per_sm"]
     assert get(pool._ctx, _lib.TUNE_SORT_ITEMS) == ch["sort_keys_per_thread"]
