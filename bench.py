@@ -72,6 +72,7 @@ def parse():
     ap.add_argument("--no-modes", action="store_true", help="skip the precision modes' step times")
     ap.add_argument("--no-sweep", action="store_true", help="serve: skip the arrival-rate sweep")
     ap.add_argument("--no-small", action="store_true", help="skip the config-0 (16384-particle) line")
+    ap.add_argument("--no-plain", action="store_true", help="batch96: skip the back-to-back plain runs")
     ap.add_argument("--requests", type=int, default=16, help="serve: requests in the stream")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrival rate (1/s)")
     ap.add_argument("--min-steps", type=int, default=100, help="serve: fewest steps of a request")
@@ -517,7 +518,7 @@ def _timed_steps(stream_ptr, local, K, step, flush):
     return [a.elapsed_time(b) for a, b in ev]
 
 
-def batch_compare(local, K, W, tune=True):
+def batch_compare(local, K, W, tune=True, plain=True):
     """Batched ensemble (one pool, one graph per step) vs the same galaxies as
     back-to-back plain runs, same GPU, same steps."""
     import torch
@@ -546,7 +547,7 @@ def batch_compare(local, K, W, tune=True):
     # the same galaxies, one after another, each in its own single-galaxy context
     pms = 0.0
     plain_steps = []
-    for g, ph in gals:
+    for g, ph in (gals if plain else []):
         sim = NBodyGPU(local, g.particles, g.stellar)
         sim.updateParams(**params_dict(g, ph))
         sf = ph.sf_eff > 0
@@ -559,7 +560,7 @@ def batch_compare(local, K, W, tune=True):
     b_total = sum(bms)
     srt = sorted(bms)
     value = Ntot * K / (b_total / 1e3)
-    plain = Ntot * K / (pms / 1e3)
+    plain = Ntot * K / (pms / 1e3) if pms else None
     return {
         "value": round(value, 1), "unit": UNIT, "steps": K, "warmup": W,
         "ms_per_step": round(b_total / K, 4),
@@ -570,8 +571,9 @@ def batch_compare(local, K, W, tune=True):
         "latency_ms": {"p50": round(srt[len(srt) // 2], 4),
                        "p99": round(srt[min(len(srt) - 1, int(0.99 * len(srt)))], 4)},
         "plain_back_to_back": {"value": round(plain, 1), "ms_per_step_all_galaxies": round(pms / K, 4),
-                               "ms_per_step_p50_galaxy": round(sorted(plain_steps)[len(plain_steps) // 2], 4)},
-        "batched_over_plain": round(value / plain, 3),
+                               "ms_per_step_p50_galaxy": round(sorted(plain_steps)[len(plain_steps) // 2], 4)}
+        if plain else None,
+        "batched_over_plain": round(value / plain, 3) if plain else None,
         "autotune": tuned,
         "finite_diagnostics": bool(torch.isfinite(torch.tensor(E)).all()),
         "clocks": clocks,
@@ -637,7 +639,8 @@ def _mode_line(d):
 def run_batch(args, ws, rank, local):
     if rank != 0:
         return
-    print(json.dumps(_mode_line(batch_compare(local, args.steps, args.warmup, tune=not args.no_tune))), flush=True)
+    print(json.dumps(_mode_line(batch_compare(local, args.steps, args.warmup, tune=not args.no_tune,
+                                              plain=not args.no_plain))), flush=True)
 
 
 def run_serve(args, ws, rank, local):
