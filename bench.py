@@ -183,6 +183,21 @@ class Clocks:
                 "reasons": reasons, "samples": len(load)}
 
 
+# Algorithmic bytes of a rebuild: bbox 16, codes 16 + 4, four sort passes of
+# 8 B read + 8 B written, gather 4 + 48 read + 48 written, tree flags / scan /
+# emit 5, leaf COM 16 per particle; per node 13 (emit) + 8 (leaf lists, an upper
+# bound) + 41 (COM cascade).
+REBUILD_BYTES_PER_PARTICLE = 16 + 20 + 64 + 100 + 5 + 16
+REBUILD_BYTES_PER_NODE = 13 + 8 + 41
+
+
+def hbm_peak():
+    """(GB/s, where it comes from): the measured copy bandwidth of this pool's B200s,
+    or the earlier measurement when the peaks file is absent."""
+    p = measured_peaks().get("hbm_gbs")
+    return (float(p), "measured (MEASURED_PEAKS.json)") if p else (6650.0, "fallback 6.65 TB/s")
+
+
 def measured_peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -272,6 +287,17 @@ def run_ours(args, ws, rank, local):
         walk_ms.append(b.elapsed_time(c))
     # median: a host stall longer than the gate leaves the device idle inside a pair
     walk_avg = statistics.median(walk_ms)
+    import ctypes as _C
+
+    nn, nl = _C.c_uint32(0), _C.c_uint32(0)
+    _lib.check(_lib.lib().gs_get_tree(sim.gpu._ctx, None, 0, _C.byref(nn), None, 0, _C.byref(nl), None), sim.gpu._ctx)
+    rb_ms = statistics.median(build_ms)
+    rbytes = N * REBUILD_BYTES_PER_PARTICLE + nn.value * REBUILD_BYTES_PER_NODE
+    hbm, hbm_src = hbm_peak()
+    rebuild = {"ms": round(rb_ms, 4), "algorithmic_bytes": int(rbytes), "nodes": int(nn.value),
+               "GBps": round(rbytes / (rb_ms / 1e3) / 1e9, 1), "peak_GBps": hbm, "peak_source": hbm_src,
+               "frac": round(rbytes / (rb_ms / 1e3) / 1e9 / hbm, 4),
+               "bytes_model": f"{REBUILD_BYTES_PER_PARTICLE} B/particle + {REBUILD_BYTES_PER_NODE} B/node"}
     fp32_peak = 148 * 128 * 2 * float(measured_peaks().get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
     achieved = interactions * FLOPS_PER_INTERACTION / (walk_avg / 1e3) / 1e12
     roofline = {"kernel": "walk_kernel (BH walk + halo + kick-drift)", "bound": "fp32",
@@ -383,7 +409,7 @@ def run_ours(args, ws, rank, local):
                        "max": round(step_sorted[-1], 5)},
         "interactions_per_particle": round(interactions / N, 2),
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-        "precision_modes": precision, "config0": small,
+        "precision_modes": precision, "config0": small, "rebuild": rebuild,
         "gpu_launches": K * n_launch_step,
         "batched": batched, "served": served, "autotune": tuned,
     }
@@ -542,6 +568,16 @@ def batch_compare(local, K, W, tune=True, plain=True):
     with Clocks(local) as clk:
         bms = _timed_steps(pool.stream, local, K, lambda: pool.run(1, True), flush)
     clocks = clk.summary()
+    # the pool's rebuild alone (codes, sort, gather, build, COM), outside the step
+    # graph, L2 flushed before each: achieved bandwidth over its algorithmic bytes
+    rb = statistics.median(_timed_steps(pool.stream, local, 10, pool.sort_build, flush))
+    nodes = sum(pool.num_nodes(sl) for sl in list(pool.n))
+    rbytes = Ntot * REBUILD_BYTES_PER_PARTICLE + nodes * REBUILD_BYTES_PER_NODE
+    peak, src = hbm_peak()
+    rebuild = {"ms": round(rb, 4), "algorithmic_bytes": int(rbytes), "nodes": int(nodes),
+               "GBps": round(rbytes / (rb / 1e3) / 1e9, 1), "peak_GBps": peak, "peak_source": src,
+               "frac": round(rbytes / (rb / 1e3) / 1e9 / peak, 4),
+               "bytes_model": f"{REBUILD_BYTES_PER_PARTICLE} B/particle + {REBUILD_BYTES_PER_NODE} B/node"}
     E = pool.energies()
     pool.close()
     # the same galaxies, one after another, each in its own single-galaxy context
@@ -574,7 +610,7 @@ def batch_compare(local, K, W, tune=True, plain=True):
                                "ms_per_step_p50_galaxy": round(sorted(plain_steps)[len(plain_steps) // 2], 4)}
         if plain else None,
         "batched_over_plain": round(value / plain, 3) if plain else None,
-        "autotune": tuned,
+        "autotune": tuned, "rebuild": rebuild,
         "finite_diagnostics": bool(torch.isfinite(torch.tensor(E)).all()),
         "clocks": clocks,
     }

@@ -58,8 +58,8 @@ struct __align__(16) SegDesc {
   uint32_t max_nodes;           // pool of MortonTree's third leaf clause (2n + 4096)
   uint32_t slot;                // index of the galaxy's DevState, TreeMeta, frame, histograms
   uint32_t diag_chunk0;         // first block of the diagnostics reduction
-  uint32_t wlpp;                 // walk lanes per particle (1, 2, 4: walk items of 32, 16, 8)
-  uint32_t pad_;
+  uint32_t wlpp;                 // walk lanes per particle (1, 2, 4, 8: items of 32, 16, 8, 4)
+  uint32_t item0;                // first walk item (diagnostic partials: groups x wlpp per galaxy)
 };
 
 // Device view of a batch's layout: segments (sorted by particle offset) and the

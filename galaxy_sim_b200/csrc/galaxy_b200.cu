@@ -425,6 +425,7 @@ int ensure_layout(gs_ctx* c) {
   std::vector<SegDesc> h(order.size());
   uint32_t st = 0, ft = 0, gr = 0, dc = 0, hs = 0;
   uint32_t items[4] = {0, 0, 0, 0};
+  uint32_t it = 0;  // walk items so far (their diagnostic partials are contiguous per galaxy)
   for (size_t r = 0; r < order.size(); r++) {
     Slot& s = c->slots[order[r]];
     s.rank = (uint32_t)r;
@@ -441,6 +442,8 @@ int ensure_layout(gs_ctx* c) {
     d.slot = order[r];
     d.diag_chunk0 = dc;
     d.wlpp = walk_lpp(c, s.n);
+    d.item0 = it;
+    it += cdiv(s.n, kWalkGroup) * d.wlpp;
     h[r] = d;
     dc += cdiv(cdiv(s.n, kWalkGroup), kDiagChunk);
     st += cdiv(s.n, (uint64_t)kSortThreads * c->sort_items);

@@ -389,7 +389,7 @@ __global__ void __launch_bounds__(32 * kPartials)
   double v = 0;
   for (uint32_t b = g0 + lane; b < g1; b += 32)
     for (uint32_t q = 0; q < sd.wlpp; q++)  // the group's work items, in order
-      v += partials[((size_t)(sd.group0 + b) * kWalkParts + q) * kPartials + k];
+      v += partials[((size_t)sd.item0 + b * sd.wlpp + q) * kPartials + k];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   if (lane == 0) chunk_part[(size_t)x * kPartials + k] = v;

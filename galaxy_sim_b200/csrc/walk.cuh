@@ -127,7 +127,7 @@ struct WalkArgs {
   float* __restrict__ energy;       // e_i
   float4* __restrict__ dbg_acc;     // optional {ax, ay, az, phi} (G applied)
   float* __restrict__ dbg_dens;
-  double* __restrict__ partials;    // [groups][kWalkParts][kPartials]
+  double* __restrict__ partials;    // [walk items][kPartials], a galaxy's from its SegDesc item0
   unsigned* work;                   // [0] next group, [1] finished warps (self-resetting)
   Layout L;                         // galaxies and the group -> galaxy map
   uint32_t pool_n, node_pool;       // particle and node pool sizes (memory-safety bounds)
@@ -614,7 +614,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
 #pragma unroll
       for (int k = 1; k < kPartials; k++)
         if (lane == k) pv = v[k];
-      a.partials[((size_t)gcur * kWalkParts + part) * kPartials + lane] = pv;
+      a.partials[((size_t)sd.item0 + (gcur - sd.group0) * LPP + part) * kPartials + lane] = pv;
     }
     if (DBG) {
 #pragma unroll

@@ -182,6 +182,13 @@ class GalaxyPool:
             nl = lr.shape[0]
         self._ok(lib().gs_upload_tree(self._ctx, ptr(nd), int(num_nodes), ptr(lr), nl))
 
+    def num_nodes(self, slot: int) -> int:
+        """Node count of one galaxy's current tree."""
+        self._sel(slot)
+        nn, nl = C.c_uint32(0), C.c_uint32(0)
+        self._ok(lib().gs_get_tree(self._ctx, None, 0, C.byref(nn), None, 0, C.byref(nl), None))
+        return nn.value
+
     def get_tree(self, slot: int, want_perm: bool = True):
         """(nodes, level ranges, permutation of the last rebuild) of one galaxy."""
         from ._lib import NODE_DTYPE
