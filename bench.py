@@ -418,7 +418,8 @@ def run_ours(args, ws, rank, local):
 
 def small_disk(local, flush, steps=50, warmup=5):
     """Config 0 (one disk of N = 16384, eps 0.05, theta 0.5, no gas): full-step and
-    walk time at each walk group size, the default (by galaxy size) first."""
+    walk time at several walk group sizes and splits, the default (both by galaxy
+    size) first."""
     import torch
 
     from galaxy_sim_b200 import _lib
@@ -428,10 +429,11 @@ def small_disk(local, flush, steps=50, warmup=5):
     w = WORKLOADS["disk16k"]
     g = w.make()
     out = {"workload": w.name, "N": int(g.N), "theta": w.physics.theta, "epsilon": w.physics.epsilon,
-           "unit": "ms", "by_group": {}}
-    for wg in (0, 8, 16, 32):
+           "unit": "ms", "by_setting": {}}
+    for wg, split in ((0, 0), (8, 1), (8, 4), (16, 2), (32, 1)):
         sim = Simulation(g, w.physics, device=local)
         set_(sim.gpu._ctx, _lib.TUNE_WALK_GROUP, wg)
+        set_(sim.gpu._ctx, _lib.TUNE_WALK_SPLIT, split)
         sim.run(warmup)
         t = _timed_steps(sim.gpu.stream, local, steps, lambda: sim.run(1), flush)
         ext = torch.cuda.ExternalStream(sim.gpu.stream, device=torch.device("cuda", local))
@@ -451,13 +453,13 @@ def small_disk(local, flush, steps=50, warmup=5):
             sim.sync()
             walk.append(b.elapsed_time(c))
         sim.close()
-        key = "by_size" if wg == 0 else str(wg)
-        out["by_group"][key] = {"ms_per_step": round(statistics.median(t), 4),
-                                "walk_ms": round(statistics.median(walk), 4)}
-    d = out["by_group"]["by_size"]
+        key = "by_size" if wg == 0 else f"group{wg}_split{split}"
+        out["by_setting"][key] = {"ms_per_step": round(statistics.median(t), 4),
+                                  "walk_ms": round(statistics.median(walk), 4)}
+    d = out["by_setting"]["by_size"]
     out["ms_per_step"], out["walk_ms"] = d["ms_per_step"], d["walk_ms"]
     out["value"] = round(g.N / (d["ms_per_step"] / 1e3), 1)
-    out["walk_group"] = "by galaxy size (8 particles at N = 16384)"
+    out["walk_group"] = "by galaxy size (8 particles per warp, each walk item split in 2, at N = 16384)"
     return out
 
 

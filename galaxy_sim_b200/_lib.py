@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libgalaxy_b200.so")
 
 GS_OK, GS_EINVAL, GS_ENOMEM, GS_ECUDA, GS_ETIMEDOUT, GS_EDEVICE, GS_ENOTREADY = 0, -1, -2, -3, -4, -5, -6
 DERR_LOOKBACK, DERR_STACK, DERR_NODES, DERR_TREE = 0x1, 0x2, 0x4, 0x8
-TUNE_WALK_BLOCKS_PER_SM, TUNE_SORT_ITEMS, TUNE_WALK_GROUP = 1, 2, 3
+TUNE_WALK_BLOCKS_PER_SM, TUNE_SORT_ITEMS, TUNE_WALK_GROUP, TUNE_WALK_SPLIT = 1, 2, 3, 4
 
 NODE_DTYPE = np.dtype([
     ("com", "<f4", (3,)), ("mass", "<f4"), ("size", "<f4"), ("isLeaf", "<u4"),

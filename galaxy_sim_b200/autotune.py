@@ -8,6 +8,11 @@ Knobs (`gs_set_tuning`):
   smaller groups to fill the GPU; large ones walk fastest in groups of 32. The
   group size changes the order of the force sums, so results change at the
   rounding level (inside the force tolerance) with it;
+* walk split: how many parts each work item's walk is split into (1, 2, 4 or
+  8, or 0 = by size) when the context walks one galaxy. A small galaxy's walk is
+  as long as its densest work item; parts walk disjoint subtrees in parallel.
+  Like the group size it changes only the order of the force sums. A pool of
+  several galaxies walks unsplit, so the tuner skips this knob there;
 * the persistent walk grid (blocks per SM; groups are independent, so fewer
   resident warps only change the schedule; below 8 the walk compiled for 72
   registers per thread runs) - never changes results;
@@ -19,7 +24,8 @@ The bucket size (16) is not a knob: it is the reference's tree
 
 ``autotune(owner)`` times a few full steps of the owner's actual workload for
 each candidate (CUDA events on the context's stream, after warm-up steps):
-first the walk group size, then the walk grid x sort tile, keeps the fastest
+first the walk group size, then the walk split, then the walk grid x sort
+tile, keeps the fastest
 and leaves it set. It advances the simulation by (warmup + steps) x candidates
 steps, so call it on a copy or accept the steps.
 """
@@ -28,11 +34,13 @@ from __future__ import annotations
 import ctypes as C
 import itertools
 
-from ._lib import TUNE_SORT_ITEMS, TUNE_WALK_BLOCKS_PER_SM, TUNE_WALK_GROUP, GalaxyError, check, lib
+from ._lib import (TUNE_SORT_ITEMS, TUNE_WALK_BLOCKS_PER_SM, TUNE_WALK_GROUP, TUNE_WALK_SPLIT, GalaxyError,
+                   check, lib)
 
 WALK_BLOCKS = (6, 7, 8)
 SORT_ITEMS = (8, 16)
 WALK_GROUPS = (0, 4, 8, 16, 32)
+WALK_SPLITS = (0, 1, 2, 4, 8)
 
 
 def get(ctx, knob: int) -> int:
@@ -61,7 +69,7 @@ def _time(owner, ext, steps, warmup, star_formation):
 
 def autotune(owner, steps: int = 5, warmup: int = 2, star_formation: bool = False,
              walk_blocks=WALK_BLOCKS, sort_items=SORT_ITEMS, walk_groups=WALK_GROUPS,
-             device: int = 0) -> dict:
+             walk_splits=WALK_SPLITS, device: int = 0) -> dict:
     """owner: an NBodyGPU or GalaxyPool (anything with ``_ctx``, ``stream`` and
     ``run(n, star_formation)``). Returns {"choice": {...}, "ms": {...}}."""
     import torch
@@ -74,6 +82,15 @@ def autotune(owner, steps: int = 5, warmup: int = 2, star_formation: bool = Fals
         group_ms[wg] = _time(owner, ext, steps, warmup, star_formation)
     best_group = min(group_ms, key=group_ms.get)
     set_(ctx, TUNE_WALK_GROUP, best_group)
+    split_ms = {}
+    if len(getattr(owner, "n", {0: 0})) == 1:   # a lone galaxy: the split applies
+        for sp in walk_splits:
+            set_(ctx, TUNE_WALK_SPLIT, sp)
+            split_ms[sp] = _time(owner, ext, steps, warmup, star_formation)
+        best_split = min(split_ms, key=split_ms.get)
+        set_(ctx, TUNE_WALK_SPLIT, best_split)
+    else:
+        best_split = get(ctx, TUNE_WALK_SPLIT)
     timing = {}
     for bps, items in itertools.product(walk_blocks, sort_items):
         try:
@@ -86,9 +103,12 @@ def autotune(owner, steps: int = 5, warmup: int = 2, star_formation: bool = Fals
     set_(ctx, TUNE_WALK_BLOCKS_PER_SM, best[0])
     set_(ctx, TUNE_SORT_ITEMS, best[1])
     return {"choice": {"walk_group": best_group if best_group else "by galaxy size",
+                       "walk_split": (best_split if best_split else "by galaxy size") if split_ms
+                       else "unsplit (several galaxies)",
                        "walk_blocks_per_sm": best[0], "sort_keys_per_thread": best[1]},
             "ms": {**{f"group{g or 'auto'}": round(t, 4) for g, t in group_ms.items()},
+                   **{f"split{p or 'auto'}": round(t, 4) for p, t in split_ms.items()},
                    **{f"{b}x{i}": round(t, 4) for (b, i), t in timing.items()}}}
 
 
-__all__ = ["autotune", "get", "set_", "WALK_BLOCKS", "SORT_ITEMS", "WALK_GROUPS"]
+__all__ = ["autotune", "get", "set_", "WALK_BLOCKS", "SORT_ITEMS", "WALK_GROUPS", "WALK_SPLITS"]

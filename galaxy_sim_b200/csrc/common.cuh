@@ -60,6 +60,8 @@ struct __align__(16) SegDesc {
   uint32_t diag_chunk0;         // first block of the diagnostics reduction
   uint32_t wlpp;                 // walk lanes per particle (1, 2, 4, 8: items of 32, 16, 8, 4)
   uint32_t item0;                // first walk item (diagnostic partials: groups x wlpp per galaxy)
+  uint32_t wsplit;               // walk splits per work item (1, 2, 4, 8; above 1 for a lone galaxy only)
+  uint32_t pad_[3];
 };
 
 // Device view of a batch's layout: segments (sorted by particle offset) and the

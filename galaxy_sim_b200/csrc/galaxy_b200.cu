@@ -222,6 +222,9 @@ struct gs_ctx {
   double* partials = nullptr;
   unsigned* walk_work = nullptr;
   uint32_t walk_grid = 0;   // persistent walk grid (largest class)
+  float4* split_buf = nullptr;       // split walk partial sums (grown on demand)
+  unsigned* split_arrive = nullptr;  // split walk arrivals per work item (zero between launches)
+  size_t split_buf_cap = 0, split_arrive_cap = 0;
   float4* dbg_acc = nullptr;
   float* dbg_dens = nullptr;
   bool debug = false;
@@ -236,6 +239,7 @@ struct gs_ctx {
   int sort_items = kSortItems;     // tuning: keys per thread of a sort tile (8 or 16)
   int walk_bps = kWalkBlocksPerSM; // tuning: persistent walk blocks per SM (1..8; < 8: 72-register build)
   int walk_group = 32;             // tuning: walk group size (0: by galaxy size; 4, 8, 16 or 32 particles)
+  int walk_split = 1;              // tuning: walk splits per work item of a lone galaxy (0: by its size; 1, 2, 4, 8)
   uint32_t walk_items[4] = {0, 0, 0, 0};  // work items per lanes-per-particle class (1, 2, 4, 8)
   bool walk_comp = false;  // Kahan-compensated far-field sums in the walk
   void* host_stage = nullptr;  // pinned: [slots] params
@@ -407,9 +411,20 @@ uint32_t walk_lpp(const gs_ctx* c, uint32_t n) {
   if (c->walk_group == 8) return 4;
   if (c->walk_group == 16) return 2;
   if (c->walk_group == 32) return 1;
-  if (n <= kWalkAuto4) return 8;
   if (n <= kWalkAuto8) return 4;
   if (n <= kWalkAuto16) return 2;
+  return 1;
+}
+
+// Walk splits per work item of a lone galaxy of n particles walked in groups of
+// lpp > 1 lanes per particle: the context's forced count, or by size (a small
+// galaxy's walk is as long as its densest work items; splitting their trees
+// shortens them). Groups of 32 (lpp 1) walk unsplit.
+uint32_t walk_split_of(const gs_ctx* c, uint32_t n, uint32_t lpp) {
+  if (lpp == 1) return 1;
+  if (c->walk_split > 0) return (uint32_t)c->walk_split;
+  if (n <= kSplitAuto4) return 4;
+  if (n <= kSplitAuto2) return 2;
   return 1;
 }
 
@@ -443,12 +458,14 @@ int ensure_layout(gs_ctx* c) {
     d.diag_chunk0 = dc;
     d.wlpp = walk_lpp(c, s.n);
     d.item0 = it;
+    d.wsplit = order.size() == 1 ? walk_split_of(c, s.n, d.wlpp) : 1;  // a pool of several fills the GPU unsplit
     it += cdiv(s.n, kWalkGroup) * d.wlpp;
     h[r] = d;
     dc += cdiv(cdiv(s.n, kWalkGroup), kDiagChunk);
     st += cdiv(s.n, (uint64_t)kSortThreads * c->sort_items);
     ft += cdiv(s.n, kFlagTile);
-    items[h[r].wlpp == 1 ? 0 : h[r].wlpp == 2 ? 1 : h[r].wlpp == 4 ? 2 : 3] += cdiv(s.n, kWalkGroup) * h[r].wlpp;
+    items[h[r].wlpp == 1 ? 0 : h[r].wlpp == 2 ? 1 : h[r].wlpp == 4 ? 2 : 3] +=
+        cdiv(s.n, kWalkGroup) * h[r].wlpp * h[r].wsplit;
     gr += cdiv(s.n, kWalkGroup);
     hs = std::max(hs, order[r] + 1);
   }
@@ -456,6 +473,23 @@ int ensure_layout(gs_ctx* c) {
       dc > c->plan.diag_chunks)
     return c->fail(GS_EINVAL, "layout exceeds the pool's tile capacity");
   CK(c, cudaStreamSynchronize(c->stream), "sync");
+  if (h.size() == 1 && h[0].wsplit > 1) {  // the split walk's sums and arrival counters
+    const size_t need = (size_t)3 * h[0].wsplit * h[0].n;
+    const size_t arr = (size_t)cdiv(h[0].n, kWalkGroup) * h[0].wlpp;
+    if (need > c->split_buf_cap) {
+      float4* p = nullptr;
+      CK(c, c->alloc(&p, need), "split walk sums");
+      c->split_buf = p;  // a smaller one stays owned until the context is destroyed
+      c->split_buf_cap = need;
+    }
+    if (arr > c->split_arrive_cap) {
+      unsigned* p = nullptr;
+      CK(c, c->alloc(&p, arr), "split walk arrivals");
+      CK(c, cudaMemset(p, 0, arr * sizeof(unsigned)), "memset");
+      c->split_arrive = p;
+      c->split_arrive_cap = arr;
+    }
+  }
   if (!h.empty()) {
     CK(c, cudaMemcpy(c->segs, h.data(), sizeof(SegDesc) * h.size(), cudaMemcpyHostToDevice), "layout");
     const uint32_t tot = std::max(st, std::max(ft, gr));
@@ -593,6 +627,10 @@ void enqueue_walk(gs_ctx* c, int sf) {
   const bool one = c->lay.nseg == 1;
   if (one) a.seg0 = c->seg_host[0];
   else memset(&a.seg0, 0, sizeof(a.seg0));
+  a.meta = c->meta;
+  a.split_buf = c->split_buf;
+  a.split_arrive = c->split_arrive;
+  a.split_stride = one ? a.seg0.n : 0u;
   const int v = (sf ? 1 : 0) | (c->debug ? 2 : 0) | (one ? 4 : 0) | (c->walk_comp ? 8 : 0);
   // one launch per walk group size present (a single galaxy: its own); 8 blocks
   // per SM: the 64-register build, fewer: the 72-register build (groups of 32)
@@ -964,6 +1002,7 @@ int gs_create_on(int device, uint32_t N, const float* particles8, const float* s
   c->single = true;
   c->walk_bps = kWalkBlocksWide;  // one galaxy: the 72-register walk measured faster
   c->walk_group = 0;              // one galaxy: walk groups by its size (a pool fills the GPU with 32s)
+  c->walk_split = 0;              // and walk splits by its size
   return GS_OK;
 }
 
@@ -1235,6 +1274,10 @@ int gs_set_tuning(gs_ctx* ctx, int knob, int value) {
     if (value != 0 && value != 4 && value != 8 && value != 16 && value != 32)
       return ctx->fail(GS_EINVAL, "walk group must be 0 (by galaxy size), 4, 8, 16 or 32 particles");
     ctx->walk_group = value;
+  } else if (knob == GS_TUNE_WALK_SPLIT) {
+    if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8)
+      return ctx->fail(GS_EINVAL, "walk split must be 0 (by galaxy size), 1, 2, 4 or 8");
+    ctx->walk_split = value;
   } else {
     return ctx->fail(GS_EINVAL, "unknown tuning knob %d", knob);
   }
@@ -1250,6 +1293,7 @@ int gs_get_tuning(gs_ctx* ctx, int knob, int* value) {
   if (knob == GS_TUNE_WALK_BLOCKS_PER_SM) *value = ctx->walk_bps;
   else if (knob == GS_TUNE_SORT_ITEMS) *value = ctx->sort_items;
   else if (knob == GS_TUNE_WALK_GROUP) *value = ctx->walk_group;
+  else if (knob == GS_TUNE_WALK_SPLIT) *value = ctx->walk_split;
   else return ctx->fail(GS_EINVAL, "unknown tuning knob %d", knob);
   return GS_OK;
 }

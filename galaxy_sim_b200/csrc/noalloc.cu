@@ -114,6 +114,8 @@ __global__ void noalloc_layout_kernel(SegDesc* seg, uint32_t* map, uint32_t N, u
     d.diag_chunk0 = 0;
     d.wlpp = 1;
     d.item0 = 0;
+    d.wsplit = 1;
+    d.pad_[0] = d.pad_[1] = d.pad_[2] = 0;
     *seg = d;
   }
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tiles; t += gridDim.x * blockDim.x) map[t] = 0;

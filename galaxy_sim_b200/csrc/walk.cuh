@@ -34,6 +34,12 @@
 //     in a pool.
 //   * Over a batch, every group belongs to one galaxy and walks that galaxy's
 //     tree with its own Params; warps steal groups across all galaxies.
+//   * Walk split (one galaxy): a small galaxy's walk is as long as its densest
+//     work item. With wsplit = S > 1 each item is walked by S warps over
+//     disjoint parts of the tree (the nodes of one level dealt out in turn, with
+//     their subtrees; the levels above belong to part 0), and the last of the S
+//     to finish adds their sums in part order and integrates. Every interaction
+//     happens once, as in the unsplit walk; only the order of the sums changes.
 #pragma once
 #include "common.cuh"
 
@@ -56,12 +62,18 @@ constexpr int kWalkBlocksWide = 7;
 constexpr uint32_t kWalkGroup = 32;             // particles per walk group (layout, diagnostics)
 constexpr uint32_t kWalkParts = 8;              // partial-sum slots per walk group (the largest LPP)
 // with the walk group chosen by size, galaxies of at most this many particles
-// walk in groups of 4 / 8 / 16 particles (measured crossovers of the step time
-// on a B200: 4 is fastest at 4096-8192 particles, 8 up to 32768, 16 at 65536,
-// 32 from 262144 on)
-constexpr uint32_t kWalkAuto4 = 12000;
+// walk in groups of 8 / 16 particles (measured crossovers of the step time on a
+// B200 with the split below: 8 is fastest up to 32768 particles, 16 at 65536,
+// 16 and 32 tie at 131072, 32 from 150000 on)
 constexpr uint32_t kWalkAuto8 = 45000;
-constexpr uint32_t kWalkAuto16 = 150000;
+constexpr uint32_t kWalkAuto16 = 100000;
+// a split walk splits at the first tree level of at least this many nodes per split
+constexpr uint32_t kSplitMinNodes = 4;
+// with the walk split chosen by size, a lone galaxy of at most this many
+// particles walks each work item in 4 / 2 parts (measured: 4 parts fastest at
+// 4096-8192 particles, 2 and 4 tie at 16384, none from 32768 on)
+constexpr uint32_t kSplitAuto4 = 12000;
+constexpr uint32_t kSplitAuto2 = 24000;
 
 // nbody_bh.wgsl:206-213
 __device__ inline uint32_t pcg(uint32_t v0) {
@@ -132,6 +144,13 @@ struct WalkArgs {
   Layout L;                         // galaxies and the group -> galaxy map
   uint32_t pool_n, node_pool;       // particle and node pool sizes (memory-safety bounds)
   SegDesc seg0;                     // the only galaxy, for the one-galaxy instantiation
+  // split walks (one galaxy, seg0.wsplit > 1): the tree levels of the split, the
+  // per-split partial sums [3][wsplit][split_stride] (float4: ax pair, ay pair;
+  // az pair, potential pair; density, self weight) and the arrivals per work item
+  const TreeMeta* meta;
+  float4* split_buf;
+  unsigned* split_arrive;           // zero between launches (the last arrival resets it)
+  uint32_t split_stride;
 };
 
 // Per-warp shared staging.
@@ -261,7 +280,10 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
                         : LPP == 4 ? (0x03030303u << (2 * sub))
                                    : (0x00030003u << (2 * sub));
   WalkSmem& S = smem_all[warp];
-  const uint32_t nitems = a.L.groups * kStride;
+  // splits per work item (1, 2, 4, 8): a lone galaxy walked in groups of 16 or
+  // fewer (the 32-particle build, the large galaxies' walk, carries no split code)
+  const uint32_t NS = ONE && LPP > 1 ? a.seg0.wsplit : 1u;
+  const uint32_t nitems = a.L.groups * kStride * NS;
   const unsigned full = 0xffffffffu;
 
   while (true) {
@@ -269,15 +291,21 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
     if (lane == 0) c = atomicAdd(&a.work[0], 1u);
     c = __shfl_sync(full, c, 0);
     if (c >= nitems) break;
-    const uint32_t gcur = c / kStride, part = c % kStride;
+    const uint32_t ksp = c % NS, cq = c / NS;  // split ksp of work item cq
+    const uint32_t gcur = cq / kStride, part = cq % kStride;
     const SegDesc sd = ONE ? a.seg0 : a.L.segs[a.L.seg_of_group[gcur]];
     if (!ONE && sd.wlpp != LPP) continue;  // a galaxy of another group size
     DevState* const sst = a.st + sd.slot;
     const gs_params& P = sst->p;  // read-only during the walk; fields loaded where used
-    const float eps2 = __ldg(&P.epsilon2);
+    const float eps2p = __ldg(&P.epsilon2);
     const float theta2 = __ldg(&P.theta) * __ldg(&P.theta);
-    const float qe2 = 0.25f * eps2;
-    const bool soft = eps2 > 0.0f;  // self pairs may then be summed and removed afterwards
+    const float qe2 = 0.25f * eps2p;
+    const bool soft = eps2p > 0.0f;  // self pairs may then be summed and removed afterwards
+    // Without softening a node test at r = 0 (a particle's own one-particle leaf)
+    // would weigh rsqrt(0) = inf by 0 (NaN): the distances add the smallest
+    // normal float instead, which moves no r^2 above 1e-30 by more than a
+    // rounding step, and such a node is opened as before.
+    const float eps2 = soft ? eps2p : 1.17549435e-38f;
     const uint32_t seg_end = sd.off + sd.n;
     const uint32_t gbeg = sd.off + (gcur - sd.group0) * kWalkGroup + part * G, gend = gbeg + G;
     const uint32_t i = gbeg + pl;
@@ -294,9 +322,31 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
     unsigned long long nmono = 0, npair = 0, nvisit = 0;
     const unsigned all = __ballot_sync(full, valid) & GMASK;  // the item's particles (lanes of share 0)
 
+    // Split walk: the first level of at least kSplitMinNodes nodes per split is
+    // the split level; split k owns its nodes j with j = k mod NS (counted from
+    // the level's start) and their subtrees, and split 0 also every contribution
+    // of the levels above, which the other splits test (to reach their own
+    // nodes) without adding.
+    uint32_t up_end = 0u, win_end = 0u;
+    bool idle = false;
+    if (NS > 1) {
+      const TreeMeta* m = a.meta + sd.slot;
+      const uint32_t nl = min(m->num_levels, (uint32_t)kDepths);
+      up_end = win_end = 0xffffffffu;
+      for (uint32_t l = 1; l < nl; l++) {
+        const uint32_t cnt = m->level_count[l];
+        if (cnt >= kSplitMinNodes * NS) {
+          up_end = sd.node_off + m->level_start[l];
+          win_end = up_end + cnt;
+          break;
+        }
+      }
+      idle = ksp > 0 && up_end == 0xffffffffu;  // no such level: split 0 walks the whole tree
+    }
+
     int sp = 0;
     if (lane == 0) S.stack[0] = make_uint2(sd.node_off, all);  // the root: range {node_off, 1}
-    sp = 1;
+    sp = idle ? 0 : 1;
     uint32_t budget = 4u * sd.node_cap + 1024u;
     while (sp > 0) {
       __syncwarp();
@@ -320,7 +370,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
       // count hold massless dummies. Massless and sub-softening children
       // (size^2 < eps^2/4, always accepted, nbody_bh.wgsl:112) get size^2 = -inf,
       // so the per-lane test is the single compare size^2 < theta^2 (r^2 + eps^2).
-      bool own = false, isleaf = false, massive = false;
+      bool own = false, isleaf = false, massive = false, skip = false;
       if (lane < 8 * kWalkRanges) {
         const int r = lane >> 3;
         const uint32_t c = lane & 7;
@@ -332,14 +382,20 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
         w.child = 0;
         w.info = kLeafBit;
         w.size = 1.f;
-        const bool real = c < rc;
+        bool real = c < rc, counted = true;
+        if (NS > 1 && real) {
+          const uint32_t node = rs + c;
+          if (node < up_end) counted = ksp == 0;                                    // levels above the split
+          else if (node < win_end && ((node - up_end) & (NS - 1)) != ksp) real = false;  // another split's
+        }
         if (real) {
           q = __ldg(&a.cm[rs + c]);
           w = a.info[rs + c];
         }
         const uint32_t wc = w.info & ~kLeafBit;
         isleaf = real && (w.info & kLeafBit);
-        massive = real && q.w != 0.0f;
+        massive = real && q.w != 0.0f && counted;
+        skip = isleaf && !counted;
         own = isleaf && q.w != 0.0f && w.child < gend && w.child + wc > gbeg;
         float s2 = w.s2;
         if (q.w == 0.0f) {  // never opened, contributes nothing (far away, massless)
@@ -352,7 +408,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
         S.cxy[st] = q.x;
         S.cxy[st + 2] = q.y;
         S.czm[st] = q.z;
-        S.czm[st + 2] = q.w;
+        S.czm[st + 2] = counted ? q.w : 0.0f;  // tested for opening, adds nothing
         S.cs2[lane] = s2;
         S.cnode[lane] = rs + c;
         S.cmeta[lane] = make_uint4(w.child, w.info,
@@ -362,6 +418,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
       const unsigned ownmask = __ballot_sync(full, own);  // leaves holding our particles
       const unsigned leafmask = __ballot_sync(full, isleaf);
       const unsigned massmask = DBG ? __ballot_sync(full, massive) : 0u;
+      const unsigned skipm = NS > 1 ? __ballot_sync(full, skip) : 0u;  // opened leaves another split sums
       __syncwarp();
       uint32_t actbits = 0, keep = 0;  // per range: this lane active; slots this lane may open
 #pragma unroll
@@ -412,10 +469,9 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
       }
       obits &= keep;
       const uint32_t om = __reduce_or_sync(full, obits);  // children opened by some lane
-      if (DBG) {
-        const uint32_t real = __popc(massmask & keep);  // keep holds this lane's slots only
-        nvisit += real;
-        nmono += real - __popc(obits);
+      if (DBG) {  // keep holds this lane's slots only
+        nvisit += __popc(massmask & keep);
+        nmono += __popc(massmask & keep & ~obits);
       }
       for (uint32_t bb = ownmask; bb; bb &= bb - 1) {  // own-leaf density (nbody_bh.wgsl:93-95)
         const uint32_t cc = __ffs(bb) - 1;
@@ -458,7 +514,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
       // opened leaves: direct sums, two sources at a time. Leaves of <= 16
       // particles get their batch entries from their slots' lanes and are staged
       // four per batch (one load round); larger ones go in chunks of 32.
-      const uint32_t leafc = om & leafmask;
+      const uint32_t leafc = om & leafmask & ~skipm;
       uint32_t big = 0;
       if (leafc) {
         bool sm = false, bg = false;
@@ -542,6 +598,69 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
         selfw += __shfl_xor_sync(full, selfw, o);
       }
     }
+    if (DBG) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        nmono += __shfl_xor_sync(full, nmono, o);
+        npair += __shfl_xor_sync(full, npair, o);
+        nvisit += __shfl_xor_sync(full, nvisit, o);
+      }
+      if (lane == 0) {
+        atomicAdd(&sst->counters[0], nmono);
+        atomicAdd(&sst->counters[1], npair);
+        atomicAdd(&sst->counters[2], nvisit);
+      }
+    }
+    if (NS > 1) {
+      // Each split leaves its sums in split_buf; the last split of the item to
+      // arrive adds them in split order (the same sums whatever the arrival order)
+      // and finishes the item. No split waits for another.
+      const uint32_t li = i - sd.off;
+      const size_t st = a.split_stride;
+      float4* const B = a.split_buf;
+      const float4 o0 = make_float4(ax.x, ax.y, ay.x, ay.y), o1 = make_float4(az.x, az.y, pt.x, pt.y);
+      const float4 o2 = make_float4(dens, selfw, 0.f, 0.f);
+      if (valid && sub == 0) {
+        B[(size_t)ksp * st + li] = o0;
+        B[(size_t)(NS + ksp) * st + li] = o1;
+        B[(size_t)(2 * NS + ksp) * st + li] = o2;
+      }
+      __threadfence();
+      __syncwarp();
+      unsigned* const arrive = a.split_arrive + (size_t)(gcur - sd.group0) * kStride + part;
+      unsigned prev = 0;
+      if (lane == 0) prev = atomicAdd(arrive, 1u);
+      prev = __shfl_sync(full, prev, 0);
+      if (prev != NS - 1) continue;  // another split finishes this item
+      __threadfence();
+      if (lane == 0) *arrive = 0u;   // every split of the item has arrived: ready for the next launch
+      if (valid && sub == 0) {
+        float4 u0 = o0, u1 = o1, u2 = o2;
+        for (uint32_t k = 0; k < NS; k++) {
+          float4 v0 = o0, v1 = o1, v2 = o2;
+          if (k != ksp) {
+            v0 = __ldcg(B + (size_t)k * st + li);
+            v1 = __ldcg(B + (size_t)(NS + k) * st + li);
+            v2 = __ldcg(B + (size_t)(2 * NS + k) * st + li);
+          }
+          if (k == 0) {
+            u0 = v0;
+            u1 = v1;
+            u2 = v2;
+          } else {
+            u0 = make_float4(u0.x + v0.x, u0.y + v0.y, u0.z + v0.z, u0.w + v0.w);
+            u1 = make_float4(u1.x + v1.x, u1.y + v1.y, u1.z + v1.z, u1.w + v1.w);
+            u2 = make_float4(fmaxf(u2.x, v2.x), u2.y + v2.y, 0.f, 0.f);  // the own leaf is found once or equal
+          }
+        }
+        ax = make_float2(u0.x, u0.y);
+        ay = make_float2(u0.z, u0.w);
+        az = make_float2(u1.x, u1.y);
+        pt = make_float2(u1.z, u1.w);
+        dens = u2.x;
+        selfw = u2.y;
+      }
+    }
     if (soft && selfw != 0.0f) pt.x -= selfw * p0.w * rsqrtf(eps2);
 
     double e_diag = 0, e_true = 0, mx = 0, my = 0, mz = 0, ms = 0;
@@ -615,19 +734,6 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
       for (int k = 1; k < kPartials; k++)
         if (lane == k) pv = v[k];
       a.partials[((size_t)sd.item0 + (gcur - sd.group0) * LPP + part) * kPartials + lane] = pv;
-    }
-    if (DBG) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        nmono += __shfl_xor_sync(full, nmono, o);
-        npair += __shfl_xor_sync(full, npair, o);
-        nvisit += __shfl_xor_sync(full, nvisit, o);
-      }
-      if (lane == 0) {
-        atomicAdd(&sst->counters[0], nmono);
-        atomicAdd(&sst->counters[1], npair);
-        atomicAdd(&sst->counters[2], nvisit);
-      }
     }
   }
   // the last warp to finish resets the work counters for the next launch

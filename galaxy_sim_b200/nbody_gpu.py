@@ -41,9 +41,12 @@ def build_params(N, *, dt, G, epsilon, theta=0.5, haloMass=0, haloA=1, gasDrag=0
 
 
 class NBodyGPU:
-    def __init__(self, device, particleData, stellarData=None, walkGroup=None):
-        """walkGroup: particles a warp walks together (8, 16, 32, or 0 = by size,
-        the default of a single-galaxy context; a pool uses 32)."""
+    def __init__(self, device, particleData, stellarData=None, walkGroup=None, walkSplit=None):
+        """walkGroup: particles a warp walks together (4, 8, 16, 32, or 0 = by
+        size, the default of a single-galaxy context; a pool uses 32).
+        walkSplit: parts each work item's walk is split into (1, 2, 4, 8, or 0 =
+        by size, the default; a pool of several galaxies walks unsplit, 1).
+        ``walkGroup=32, walkSplit=1`` gives a galaxy a pool's arithmetic."""
         P = f32(particleData).ravel()
         if P.size % 8:
             raise ValueError("particleData must hold 8 floats per particle")
@@ -58,10 +61,12 @@ class NBodyGPU:
         self.ready = True
         self.levelRanges = None
         self._params = GsParams()
-        if walkGroup is not None:
-            from ._lib import TUNE_WALK_GROUP
+        from ._lib import TUNE_WALK_GROUP, TUNE_WALK_SPLIT
 
+        if walkGroup is not None:
             self._ok(lib().gs_set_tuning(self._ctx, TUNE_WALK_GROUP, int(walkGroup)))
+        if walkSplit is not None:
+            self._ok(lib().gs_set_tuning(self._ctx, TUNE_WALK_SPLIT, int(walkSplit)))
 
     # -- reference surface --------------------------------------------------------------
     def _ok(self, rc):

@@ -122,16 +122,25 @@ int gs_set_walk_mode(gs_ctx* ctx, int compensated);
  * changes results (a stable sort has one answer).
  * GS_TUNE_WALK_GROUP = particles a warp walks together: 32 (one lane per particle),
  * 16, 8 or 4 (two, four or eight lanes per particle, splitting its node tests and
- * leaf sources), or 0 = by each galaxy's size (4 up to 12000 particles, 8 up to
- * 45000, 16 up to 150000, else 32). Default: 0 for a gs_create context (a small galaxy alone needs
+ * leaf sources), or 0 = by each galaxy's size (8 up to 45000 particles, 16 up to
+ * 100000, else 32). Default: 0 for a gs_create context (a small galaxy alone needs
  * the smaller groups to fill the GPU), 32 for a pool (many galaxies fill it; 32
  * costs the fewest instructions). The split changes the order of the force sums,
  * so results differ at the rounding level (inside the force tolerance) between
  * group sizes; with the same setting a galaxy gets the same result alone or
- * pooled. */
+ * pooled.
+ * GS_TUNE_WALK_SPLIT = parts each work item's walk is split into when the context
+ * walks one galaxy in groups of 16 or fewer particles (1, 2, 4 or 8, or 0 = by
+ * its size: 4 up to 12000 particles, 2 up to 24000, else 1). The parts walk
+ * disjoint subtrees in parallel and the last to finish adds their sums in a
+ * fixed order, so a small galaxy's walk is less bound by its densest work
+ * items. Default: 0 for a gs_create context, 1 for a pool; groups of 32 and a
+ * pool holding more than one galaxy always walk unsplit. Like the group size it
+ * changes only the order of the force sums. */
 #define GS_TUNE_WALK_BLOCKS_PER_SM 1
 #define GS_TUNE_SORT_ITEMS 2
 #define GS_TUNE_WALK_GROUP 3
+#define GS_TUNE_WALK_SPLIT 4
 int gs_set_tuning(gs_ctx* ctx, int knob, int value);
 int gs_get_tuning(gs_ctx* ctx, int knob, int* value);
 /* NBodyGPU.updateCentralMass (NBodyGPU.js:245-251): both ping-pong buffers. */

@@ -66,7 +66,7 @@ def test_degenerate_inputs(gpu_lib, oracle, make):
     if make is _outlier:
         assert big > 16  # the large-leaf path ran
     # full steps alone vs in a pool next to another galaxy
-    solo = NBodyGPU(0, P0, S0, walkGroup=32)   # a pool's default walk group
+    solo = NBodyGPU(0, P0, S0, walkGroup=32, walkSplit=1)   # a pool's default walk group
     solo.updateParams(**KW)
     solo.run(3, True)
     want_P, _ = solo.readState()

@@ -39,8 +39,8 @@ def _tracking(g):
     return (c1, c2, hc[0] if len(hc) > 0 else None, hc[1] if len(hc) > 1 else None)
 
 
-def _solo(g, ph, steps, sf, walk_group=32):
-    sim = NBodyGPU(0, g.particles, g.stellar, walkGroup=walk_group)  # the pool's setting
+def _solo(g, ph, steps, sf, walk_group=32, walk_split=1):
+    sim = NBodyGPU(0, g.particles, g.stellar, walkGroup=walk_group, walkSplit=walk_split)  # the pool's setting
     sim.updateParams(**params_dict(g, ph))
     t = _tracking(g)
     if t is not None:
@@ -101,6 +101,32 @@ def test_batch_equals_solo_with_walk_groups_by_size(gpu_lib):
     pool.run(steps, True)
     for s, solo in zip(slots, solos):
         _check_same(pool, s, solo)
+    pool.close()
+
+
+def test_walk_split_applies_to_a_lone_galaxy_only(gpu_lib):
+    """The split knob splits the walk of a pool holding one galaxy (the same bits
+    as a solo run with that split); a pool of several galaxies walks unsplit
+    whatever the knob says (the same bits as unsplit solo runs)."""
+    from galaxy_sim_b200 import _lib
+
+    cases = _cases()[:2]
+    steps = 2
+    pool = GalaxyPool(sum(g.N + 256 for g, _ in cases) + 4096, 4)
+    _lib.check(_lib.lib().gs_set_tuning(pool._ctx, _lib.TUNE_WALK_GROUP, 8), pool._ctx)
+    _lib.check(_lib.lib().gs_set_tuning(pool._ctx, _lib.TUNE_WALK_SPLIT, 4), pool._ctx)
+    g, ph = cases[1]
+    s1 = pool.add(g.particles, g.stellar, params_dict(g, ph), _tracking(g))
+    pool.run(steps, True)
+    split = _solo(g, ph, steps, True, walk_group=8, walk_split=4)
+    unsplit = _solo(g, ph, steps, True, walk_group=8, walk_split=1)
+    assert not np.array_equal(split[0].view(np.uint32), unsplit[0].view(np.uint32))  # the split was taken
+    _check_same(pool, s1, split)
+    pool.remove(s1)
+    slots = [pool.add(g.particles, g.stellar, params_dict(g, ph), _tracking(g)) for g, ph in cases]
+    pool.run(steps, True)
+    for s, (g, ph) in zip(slots, cases):
+        _check_same(pool, s, _solo(g, ph, steps, True, walk_group=8, walk_split=1))
     pool.close()
 
 
@@ -170,7 +196,7 @@ def test_batch_equals_solo_in_precision_modes(gpu_lib, comp, com64):
     steps = 2
     solos = []
     for g, ph in cases:
-        sim = NBodyGPU(0, g.particles, g.stellar, walkGroup=32)   # the pool's walk group
+        sim = NBodyGPU(0, g.particles, g.stellar, walkGroup=32, walkSplit=1)   # the pool's walk group
         sim.updateParams(**params_dict(g, ph))
         t = _tracking(g)
         if t is not None:

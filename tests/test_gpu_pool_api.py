@@ -24,7 +24,7 @@ def _same(a, b):
 
 
 def _solo_run(g, kw, steps):
-    sim = NBodyGPU(0, g.particles, g.stellar, walkGroup=32)
+    sim = NBodyGPU(0, g.particles, g.stellar, walkGroup=32, walkSplit=1)
     sim.updateParams(**kw)
     sim.run(steps, True)
     P, S = sim.readState()
@@ -73,7 +73,7 @@ def test_reference_flow_on_a_pool_slot(gpu_lib):
     tree = boot["tree"]
     kw = dict(dt=0.005, G=1.0, epsilon=0.05, theta=0.5, haloMass=g.halo_mass, haloA=g.halo_a,
               haloCenters=[[0, 0, 0, 0]])
-    sim = NBodyGPU(0, boot["sorted"], boot["sortedStellar"], walkGroup=32)
+    sim = NBodyGPU(0, boot["sorted"], boot["sortedStellar"], walkGroup=32, walkSplit=1)
     sim.uploadBHTree(tree.nodes, tree.numNodes, tree.levelRanges)
     sim.updateParams(**kw)
     sim.encodeRefresh()
@@ -98,7 +98,7 @@ def test_reference_flow_on_a_pool_slot(gpu_lib):
 
 def test_get_tree_on_a_pool_slot(gpu_lib):
     a, b = ic.galaxy_disk(3000, 4), ic.galaxy_disk(20000, 5)
-    sim = NBodyGPU(0, b.particles, b.stellar, walkGroup=32)
+    sim = NBodyGPU(0, b.particles, b.stellar, walkGroup=32, walkSplit=1)
     sim.sortBuild()
     want_nodes, want_lr, want_perm = sim.getTree()
     sim.destroy()

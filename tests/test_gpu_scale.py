@@ -58,7 +58,7 @@ def test_batch96_pool_equals_solo_and_forces_within_tolerance(gpu_lib, oracle):
     assert None not in slots
     pool.run(steps, True)
     for (g, ph), s in zip(gals, slots):
-        solo = NBodyGPU(0, g.particles, g.stellar, walkGroup=32)   # the pool's walk group
+        solo = NBodyGPU(0, g.particles, g.stellar, walkGroup=32, walkSplit=1)   # the pool's walk group
         solo.updateParams(**params_dict(g, ph))
         solo.run(steps, ph.sf_eff > 0)
         SP, SS = solo.readState()
@@ -129,7 +129,7 @@ def test_served_stream_at_request_scale_equals_alone(gpu_lib):
     assert stats["particle_steps"] == sum(r.N * r.steps for r in reqs)
     assert max(r.admitted - r.arrival for r in reqs) > 0     # the pool could not hold them all
     for r in reqs:
-        sim = NBodyGPU(0, r.particles, r.stellar, walkGroup=32)   # the pool's walk group
+        sim = NBodyGPU(0, r.particles, r.stellar, walkGroup=32, walkSplit=1)   # the pool's walk group
         sim.updateParams(**r.params)
         if r.tracking is not None:
             sim.setTracking(*r.tracking)

@@ -17,8 +17,8 @@ from galaxy_sim_b200.serve import BatchServer, PlainServer, make_stream
 pytestmark = pytest.mark.gpu
 
 
-def _alone(r, walk_group=None):
-    sim = NBodyGPU(0, r.particles, r.stellar, walkGroup=walk_group)
+def _alone(r, walk_group=None, walk_split=None):
+    sim = NBodyGPU(0, r.particles, r.stellar, walkGroup=walk_group, walkSplit=walk_split)
     sim.updateParams(**r.params)
     if r.tracking is not None:
         sim.setTracking(*r.tracking)
@@ -40,7 +40,7 @@ def test_served_results_equal_alone(gpu_lib):
     # the pool held at most three galaxies: some requests had to wait
     assert max(r.admitted - r.arrival for r in reqs) > 0
     for r in reqs:
-        P, S, e = _alone(r, walk_group=32)   # the pool's walk group
+        P, S, e = _alone(r, walk_group=32, walk_split=1)   # the pool's walk group, unsplit
         RP, RS, re_ = r.result
         assert np.array_equal(RP.view(np.uint32), P.view(np.uint32)), r.rid
         assert np.array_equal(RS.view(np.uint32), S.view(np.uint32)), r.rid
