@@ -644,7 +644,7 @@ void enqueue_walk(gs_ctx* c, int sf) {
     else launch_walk<kWalkBlocksWide, 1>(v, gk, s, a);
   }
   // per-galaxy FP64 diagnostics of this walk
-  launch_pdl(diag_reduce_kernel, c->lay.diag_chunks, dim3(32, kPartials), s, (const double*)c->partials, c->lay,
+  launch_pdl(diag_reduce_kernel, c->lay.diag_chunks, 32 * kPartials, s, (const double*)c->partials, c->lay,
              c->diag_chunk, c->diag_ctr, c->diag_out);
   c->cur ^= 1;
 }

@@ -365,16 +365,21 @@ __global__ void upload_convert_kernel(const gs_node* __restrict__ nodes, uint32_
 
 // FP64 diagnostics: fold each galaxy's per-item walk partials into
 // out[slot][kPartials]. A block of 32 x kPartials threads sums kDiagChunk groups
-// of one galaxy (chunks counted from the galaxy's first group); the galaxy's
-// last block adds the chunk sums in chunk order, so the result does not depend
-// on the layout or on block timing. diag_ctr[slot] self-resets.
-constexpr uint32_t kDiagChunk = 512;
+// of one galaxy (chunks counted from the galaxy's first group): the chunk's
+// partials are one contiguous run of doubles, read coalesced with a stride of
+// 32 x kPartials so that thread t always adds component t mod kPartials; the 32
+// threads of a component are then added in thread order. The galaxy's last
+// block adds the chunk sums in chunk order the same way, so the result does not
+// depend on the layout or on block timing. diag_ctr[slot] self-resets.
+constexpr uint32_t kDiagChunk = 64;
 __global__ void __launch_bounds__(32 * kPartials)
     diag_reduce_kernel(const double* __restrict__ partials, Layout L, double* chunk_part,
                        unsigned* diag_ctr, double* out) {
   griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
+  constexpr uint32_t kThreads = 32 * kPartials;
+  __shared__ double s_v[kThreads];
   __shared__ bool s_last;
-  const uint32_t x = blockIdx.x;
+  const uint32_t x = blockIdx.x, t = threadIdx.x;
   uint32_t lo = 0, hi = L.nseg;
   while (hi - lo > 1) {
     const uint32_t mid = (lo + hi) >> 1;
@@ -385,26 +390,38 @@ __global__ void __launch_bounds__(32 * kPartials)
   const uint32_t ng = (sd.n + kWalkGroup - 1) / kWalkGroup;
   const uint32_t nch = (ng + kDiagChunk - 1) / kDiagChunk;
   const uint32_t g0 = (x - sd.diag_chunk0) * kDiagChunk, g1 = min(ng, g0 + kDiagChunk);
-  const int k = threadIdx.y, lane = threadIdx.x;
+  // the chunk's work items (groups in order, each group's items in order)
+  const size_t f0 = ((size_t)sd.item0 + (size_t)g0 * sd.wlpp) * kPartials;
+  const size_t f1 = ((size_t)sd.item0 + (size_t)g1 * sd.wlpp) * kPartials;
   double v = 0;
-  for (uint32_t b = g0 + lane; b < g1; b += 32)
-    for (uint32_t q = 0; q < sd.wlpp; q++)  // the group's work items, in order
-      v += partials[((size_t)sd.item0 + b * sd.wlpp + q) * kPartials + k];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if (lane == 0) chunk_part[(size_t)x * kPartials + k] = v;
+#pragma unroll 4
+  for (size_t f = f0 + t; f < f1; f += kThreads) v += partials[f];
+  s_v[t] = v;
+  __syncthreads();
+  if (t < kPartials) {
+    double w = 0;
+    for (uint32_t j = 0; j < 32; j++) w += s_v[j * kPartials + t];
+    chunk_part[(size_t)x * kPartials + t] = w;
+  }
   __threadfence();
   __syncthreads();
-  if (lane == 0 && k == 0) s_last = atomicAdd(&diag_ctr[sd.slot], 1u) == nch - 1;
+  if (t == 0) s_last = atomicAdd(&diag_ctr[sd.slot], 1u) == nch - 1;
   __syncthreads();
   if (!s_last) return;
   __threadfence();
+  // component t mod kPartials of chunks j, j + 32, ... (j = t / kPartials)
   double w = 0;
-  for (uint32_t c = lane; c < nch; c += 32) w += __ldcg(&chunk_part[(size_t)(sd.diag_chunk0 + c) * kPartials + k]);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
-  if (lane == 0) out[(size_t)sd.slot * kPartials + k] = w;
-  if (lane == 0 && k == 0) diag_ctr[sd.slot] = 0;
+  for (uint32_t c = t / kPartials; c < nch; c += 32)
+    w += __ldcg(&chunk_part[(size_t)(sd.diag_chunk0 + c) * kPartials + t % kPartials]);
+  __syncthreads();
+  s_v[t] = w;
+  __syncthreads();
+  if (t < kPartials) {
+    double u = 0;
+    for (uint32_t j = 0; j < 32; j++) u += s_v[j * kPartials + t];
+    out[(size_t)sd.slot * kPartials + t] = u;
+  }
+  if (t == 0) diag_ctr[sd.slot] = 0;
 }
 
 // Tile / group -> galaxy maps of a layout (binary search over the galaxies'

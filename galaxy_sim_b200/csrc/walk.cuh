@@ -242,6 +242,14 @@ __device__ inline float set_gt(float a, float b) {
   return r;
 }
 
+// All ones if !(a > b) (a <= b or unordered), else 0, as one compare-and-set:
+// the open bit of a node whose weight set_gt(a, b) is 0.
+__device__ inline uint32_t set_leu(float a, float b) {
+  uint32_t r;
+  asm("set.leu.u32.f32 %0, %1, %2;" : "=r"(r) : "f"(a), "f"(b));
+  return r;
+}
+
 // Transpose of the 32 x 32 bit matrix held one row per lane: afterwards bit j
 // of lane i is bit i of lane j (five butterfly stages of 16, 8, 4, 2, 1 bits).
 __device__ __forceinline__ uint32_t warp_transpose(uint32_t x, int lane) {
@@ -451,7 +459,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
         const float2 d2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __ffma2_rn(rz, rz, f2(eps2))));
         const float2 td = __fmul2_rn(f2(t2), d2);
         const float2 w = make_float2(set_gt(td.x, s2.x), set_gt(td.y, s2.y));
-        obits |= ((w.x == 0.0f ? 1u : 0u) | (w.y == 0.0f ? 2u : 0u)) << c;
+        obits |= (set_leu(td.x, s2.x) & (1u << c)) | (set_leu(td.y, s2.y) & (2u << c));  // w == 0
         const float2 rinv = __fmul2_rn(make_float2(rsqrtf(d2.x), rsqrtf(d2.y)), w);
         const float2 mr = __fmul2_rn(qm, rinv);
         const float2 f = __fmul2_rn(__fmul2_rn(mr, rinv), rinv);
