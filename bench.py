@@ -423,7 +423,7 @@ def small_disk(local, flush, steps=50, warmup=5):
     import torch
 
     from galaxy_sim_b200 import _lib
-    from galaxy_sim_b200.autotune import set_
+    from galaxy_sim_b200.autotune import launch_setting, set_
     from galaxy_sim_b200.simulation import WORKLOADS, Simulation
 
     w = WORKLOADS["disk16k"]
@@ -434,6 +434,8 @@ def small_disk(local, flush, steps=50, warmup=5):
         sim = Simulation(g, w.physics, device=local)
         set_(sim.gpu._ctx, _lib.TUNE_WALK_GROUP, wg)
         set_(sim.gpu._ctx, _lib.TUNE_WALK_SPLIT, split)
+        if wg == 0:
+            out["setting_in_effect"] = launch_setting(sim.gpu._ctx)
         sim.run(warmup)
         t = _timed_steps(sim.gpu.stream, local, steps, lambda: sim.run(1), flush)
         ext = torch.cuda.ExternalStream(sim.gpu.stream, device=torch.device("cuda", local))
@@ -459,7 +461,10 @@ def small_disk(local, flush, steps=50, warmup=5):
     d = out["by_setting"]["by_size"]
     out["ms_per_step"], out["walk_ms"] = d["ms_per_step"], d["walk_ms"]
     out["value"] = round(g.N / (d["ms_per_step"] / 1e3), 1)
-    out["walk_group"] = "by galaxy size (8 particles per warp, each walk item split in 2, at N = 16384)"
+    eff = out["setting_in_effect"]
+    out["walk_group"] = (f"by galaxy size ({eff['walk_group']} particles per warp, walk items in "
+                         f"{eff['walk_split']} parts, {eff['sort_keys_per_thread']} sort keys per thread)")
+    out["walk_ms_includes"] = "walk kernel + FP64 diagnostics reduction (one gs_step)"
     return out
 
 

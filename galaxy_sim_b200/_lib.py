@@ -66,6 +66,7 @@ SIGNATURES = [
     ("gs_set_walk_mode", _int, [_vp, _int]),
     ("gs_set_tuning", _int, [_vp, _int, _int]),
     ("gs_get_tuning", _int, [_vp, _int, _vp]),
+    ("gs_get_launch_setting", _int, [_vp, _vp, _vp, _vp]),
     ("gs_update_central_mass", _int, [_vp, _f32, _u32]),
     ("gs_apply_permutation", _int, [_vp, _vp]),
     ("gs_upload_tree", _int, [_vp, _vp, _u32, _vp, _u32]),

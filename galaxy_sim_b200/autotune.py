@@ -16,8 +16,9 @@ Knobs (`gs_set_tuning`):
 * the persistent walk grid (blocks per SM; groups are independent, so fewer
   resident warps only change the schedule; below 8 the walk compiled for 72
   registers per thread runs) - never changes results;
-* the sort tile depth (8 or 16 keys per thread: tiles of 2048 or 4096 keys; a
-  stable sort has one answer) - never changes results.
+* the sort tile depth (4, 8 or 16 keys per thread: tiles of 1024, 2048 or 4096
+  keys; a small galaxy sorts in more tiles with the smaller depths; a stable
+  sort has one answer) - never changes results.
 
 The bucket size (16) is not a knob: it is the reference's tree
 (mortonTree.js:25), and changing it would change every result.
@@ -38,7 +39,7 @@ from ._lib import (TUNE_SORT_ITEMS, TUNE_WALK_BLOCKS_PER_SM, TUNE_WALK_GROUP, TU
                    check, lib)
 
 WALK_BLOCKS = (6, 7, 8)
-SORT_ITEMS = (8, 16)
+SORT_ITEMS = (4, 8, 16)
 WALK_GROUPS = (0, 4, 8, 16, 32)
 WALK_SPLITS = (0, 1, 2, 4, 8)
 
@@ -51,6 +52,14 @@ def get(ctx, knob: int) -> int:
 
 def set_(ctx, knob: int, value: int) -> None:
     check(lib().gs_set_tuning(ctx, knob, int(value)), ctx)
+
+
+def launch_setting(ctx) -> dict:
+    """The setting in effect for the context's selected galaxy after the "by
+    size" rules: particles per walk group, walk parts per item, sort keys per thread."""
+    g, s, i = C.c_uint32(0), C.c_uint32(0), C.c_uint32(0)
+    check(lib().gs_get_launch_setting(ctx, C.byref(g), C.byref(s), C.byref(i)), ctx)
+    return {"walk_group": g.value, "walk_split": s.value, "sort_keys_per_thread": i.value}
 
 
 def _time(owner, ext, steps, warmup, star_formation):
@@ -83,7 +92,8 @@ def autotune(owner, steps: int = 5, warmup: int = 2, star_formation: bool = Fals
     best_group = min(group_ms, key=group_ms.get)
     set_(ctx, TUNE_WALK_GROUP, best_group)
     split_ms = {}
-    if len(getattr(owner, "n", {0: 0})) == 1:   # a lone galaxy: the split applies
+    lone = len(getattr(owner, "n", {0: 0})) == 1
+    if lone and launch_setting(ctx)["walk_group"] < 32:   # the split applies
         for sp in walk_splits:
             set_(ctx, TUNE_WALK_SPLIT, sp)
             split_ms[sp] = _time(owner, ext, steps, warmup, star_formation)
@@ -104,11 +114,11 @@ def autotune(owner, steps: int = 5, warmup: int = 2, star_formation: bool = Fals
     set_(ctx, TUNE_SORT_ITEMS, best[1])
     return {"choice": {"walk_group": best_group if best_group else "by galaxy size",
                        "walk_split": (best_split if best_split else "by galaxy size") if split_ms
-                       else "unsplit (several galaxies)",
+                       else "unsplit (groups of 32)" if lone else "unsplit (several galaxies)",
                        "walk_blocks_per_sm": best[0], "sort_keys_per_thread": best[1]},
             "ms": {**{f"group{g or 'auto'}": round(t, 4) for g, t in group_ms.items()},
                    **{f"split{p or 'auto'}": round(t, 4) for p, t in split_ms.items()},
                    **{f"{b}x{i}": round(t, 4) for (b, i), t in timing.items()}}}
 
 
-__all__ = ["autotune", "get", "set_", "WALK_BLOCKS", "SORT_ITEMS", "WALK_GROUPS", "WALK_SPLITS"]
+__all__ = ["autotune", "get", "set_", "launch_setting", "WALK_BLOCKS", "SORT_ITEMS", "WALK_GROUPS", "WALK_SPLITS"]

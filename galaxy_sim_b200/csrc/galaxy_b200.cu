@@ -236,7 +236,8 @@ struct gs_ctx {
   uint32_t sel = 0;
   bool single = false;  // created by gs_create: one galaxy, node pool 2N + 4096
   int com_mode = kComF32;
-  int sort_items = kSortItems;     // tuning: keys per thread of a sort tile (8 or 16)
+  int sort_items = kSortItems;     // tuning: keys per thread of a sort tile (0: by galaxy size; 4, 8 or 16)
+  int sort_eff = kSortItems;       // the layout's keys per thread (sort_items, or chosen by size)
   int walk_bps = kWalkBlocksPerSM; // tuning: persistent walk blocks per SM (1..8; < 8: 72-register build)
   int walk_group = 32;             // tuning: walk group size (0: by galaxy size; 4, 8, 16 or 32 particles)
   int walk_split = 1;              // tuning: walk splits per work item of a lone galaxy (0: by its size; 1, 2, 4, 8)
@@ -428,6 +429,16 @@ uint32_t walk_split_of(const gs_ctx* c, uint32_t n, uint32_t lpp) {
   return 1;
 }
 
+// Sort keys per thread of a lone galaxy of n particles with the tile depth chosen
+// by size: a small galaxy sorts in more, smaller tiles (measured on a B200: 4
+// keys per thread fastest up to 65536 particles, 8 at 262144, 16 at 524288).
+int sort_items_of(const gs_ctx* c, uint32_t n) {
+  if (c->sort_items > 0) return c->sort_items;
+  if (n <= kSortAuto4) return 4;
+  if (n <= kSortAuto8) return 8;
+  return 16;
+}
+
 // Rebuild the device layout (galaxies in offset order, tile/group maps) after
 // slots were added or removed. The stream must be idle (no step in flight).
 int ensure_layout(gs_ctx* c) {
@@ -441,6 +452,9 @@ int ensure_layout(gs_ctx* c) {
   uint32_t st = 0, ft = 0, gr = 0, dc = 0, hs = 0;
   uint32_t items[4] = {0, 0, 0, 0};
   uint32_t it = 0;  // walk items so far (their diagnostic partials are contiguous per galaxy)
+  uint32_t nmax = 0;
+  for (uint32_t s : order) nmax = std::max(nmax, c->slots[s].n);
+  const int items_eff = sort_items_of(c, nmax);
   for (size_t r = 0; r < order.size(); r++) {
     Slot& s = c->slots[order[r]];
     s.rank = (uint32_t)r;
@@ -462,7 +476,7 @@ int ensure_layout(gs_ctx* c) {
     it += cdiv(s.n, kWalkGroup) * d.wlpp;
     h[r] = d;
     dc += cdiv(cdiv(s.n, kWalkGroup), kDiagChunk);
-    st += cdiv(s.n, (uint64_t)kSortThreads * c->sort_items);
+    st += cdiv(s.n, (uint64_t)kSortThreads * items_eff);
     ft += cdiv(s.n, kFlagTile);
     items[h[r].wlpp == 1 ? 0 : h[r].wlpp == 2 ? 1 : h[r].wlpp == 4 ? 2 : 3] +=
         cdiv(s.n, kWalkGroup) * h[r].wlpp * h[r].wsplit;
@@ -509,6 +523,7 @@ int ensure_layout(gs_ctx* c) {
   L.diag_chunks = dc;
   c->hist_slots = hs;
   c->seg_host = h;
+  c->sort_eff = items_eff;
   const uint32_t most = std::max(std::max(items[0], items[1]), std::max(items[2], items[3]));
   c->walk_grid = std::min<uint32_t>(std::max<uint32_t>(1, cdiv(most, kWalkWarps)), (uint32_t)c->sms * c->walk_bps);
   for (int k = 0; k < 4; k++) c->walk_items[k] = items[k];
@@ -559,7 +574,8 @@ void sort_passes_items(gs_ctx* c, bool inv, uint32_t spin_limit, uint32_t withho
 // spin_limit / withhold: the look-back wait's failure-detection test settings
 // (production: kSpinLimit, no withheld tile).
 void enqueue_sort_passes(gs_ctx* c, bool inv, uint32_t spin_limit = kSpinLimit, uint32_t withhold = kNoTile) {
-  if (c->sort_items == 8) sort_passes_items<8>(c, inv, spin_limit, withhold);
+  if (c->sort_eff == 4) sort_passes_items<4>(c, inv, spin_limit, withhold);
+  else if (c->sort_eff == 8) sort_passes_items<8>(c, inv, spin_limit, withhold);
   else sort_passes_items<16>(c, inv, spin_limit, withhold);
 }
 
@@ -1003,6 +1019,7 @@ int gs_create_on(int device, uint32_t N, const float* particles8, const float* s
   c->walk_bps = kWalkBlocksWide;  // one galaxy: the 72-register walk measured faster
   c->walk_group = 0;              // one galaxy: walk groups by its size (a pool fills the GPU with 32s)
   c->walk_split = 0;              // and walk splits by its size
+  c->sort_items = 0;              // and sort tiles by its size
   return GS_OK;
 }
 
@@ -1268,7 +1285,8 @@ int gs_set_tuning(gs_ctx* ctx, int knob, int value) {
       return ctx->fail(GS_EINVAL, "walk blocks per SM must be in [1, %d]", kWalkBlocksPerSM);
     ctx->walk_bps = value;
   } else if (knob == GS_TUNE_SORT_ITEMS) {
-    if (value != 8 && value != 16) return ctx->fail(GS_EINVAL, "sort keys per thread must be 8 or 16");
+    if (value != 0 && value != 4 && value != 8 && value != 16)
+      return ctx->fail(GS_EINVAL, "sort keys per thread must be 0 (by galaxy size), 4, 8 or 16");
     ctx->sort_items = value;
   } else if (knob == GS_TUNE_WALK_GROUP) {
     if (value != 0 && value != 4 && value != 8 && value != 16 && value != 32)
@@ -1295,6 +1313,18 @@ int gs_get_tuning(gs_ctx* ctx, int knob, int* value) {
   else if (knob == GS_TUNE_WALK_GROUP) *value = ctx->walk_group;
   else if (knob == GS_TUNE_WALK_SPLIT) *value = ctx->walk_split;
   else return ctx->fail(GS_EINVAL, "unknown tuning knob %d", knob);
+  return GS_OK;
+}
+
+int gs_get_launch_setting(gs_ctx* ctx, uint32_t* group, uint32_t* split, uint32_t* sort_items) {
+  CTX_CHECK(ctx);
+  SLOT(ctx, s);
+  int rc = ensure_layout(ctx);
+  if (rc) return rc;
+  const SegDesc& d = ctx->seg_host[s->rank];
+  if (group) *group = kWalkGroup / d.wlpp;
+  if (split) *split = d.wsplit;
+  if (sort_items) *sort_items = (uint32_t)ctx->sort_eff;
   return GS_OK;
 }
 

@@ -17,7 +17,11 @@ constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortItems = 16;                        // default keys per thread
 constexpr int kSortTile = kSortThreads * kSortItems;  // default keys per tile (4096)
-constexpr int kSortTileMin = kSortThreads * 8;        // smallest tile the runtime selects
+constexpr int kSortTileMin = kSortThreads * 4;        // smallest tile the runtime selects
+// with the tile depth chosen by size, galaxies of at most this many particles
+// sort with 4 / 8 keys per thread
+constexpr uint32_t kSortAuto4 = 131072;
+constexpr uint32_t kSortAuto8 = 393216;
 constexpr int kSortPasses = 4;                        // 30-bit codes, 8-bit digits
 constexpr uint32_t kLbAgg = 1u << 30;
 constexpr uint32_t kLbInc = 2u << 30;

@@ -118,7 +118,9 @@ int gs_set_walk_mode(gs_ctx* ctx, int compensated);
  * GS_TUNE_WALK_BLOCKS_PER_SM = persistent walk blocks per SM (1..8; default 7 for a
  * gs_create context, 8 for a pool; below 8 the walk built for 72 registers per
  * thread runs); never changes results.
- * GS_TUNE_SORT_ITEMS = keys per thread of a sort tile (8 or 16, default 16); never
+ * GS_TUNE_SORT_ITEMS = keys per thread of a sort tile (4, 8 or 16, or 0 = by the
+ * largest galaxy's size: 4 up to 131072 particles, 8 up to 393216, else 16;
+ * default 0 for a gs_create context, 16 for a pool); never
  * changes results (a stable sort has one answer).
  * GS_TUNE_WALK_GROUP = particles a warp walks together: 32 (one lane per particle),
  * 16, 8 or 4 (two, four or eight lanes per particle, splitting its node tests and
@@ -143,6 +145,10 @@ int gs_set_walk_mode(gs_ctx* ctx, int compensated);
 #define GS_TUNE_WALK_SPLIT 4
 int gs_set_tuning(gs_ctx* ctx, int knob, int value);
 int gs_get_tuning(gs_ctx* ctx, int knob, int* value);
+/* The launch setting in effect for the selected galaxy after the knobs' "by size"
+ * rules: particles per walk group (4, 8, 16, 32), walk parts per work item (1, 2,
+ * 4, 8) and sort keys per thread (4, 8, 16). Any pointer may be NULL. */
+int gs_get_launch_setting(gs_ctx* ctx, uint32_t* group, uint32_t* split, uint32_t* sort_items);
 /* NBodyGPU.updateCentralMass (NBodyGPU.js:245-251): both ping-pong buffers. */
 int gs_update_central_mass(gs_ctx* ctx, float mass, uint32_t idx);
 /* NBodyGPU.applyPermutation (NBodyGPU.js:225-238): gather out[i] = in[perm[i]] of

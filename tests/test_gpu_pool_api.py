@@ -33,7 +33,7 @@ def _solo_run(g, kw, steps):
     return P, S, e
 
 
-@pytest.mark.parametrize("sort_items", [16, 8])
+@pytest.mark.parametrize("sort_items", [16, 8, 4])
 def test_tile_edge_sizes_equal_solo(gpu_lib, sort_items):
     gals = [ic.galaxy_disk(n, 100 + k, gas_frac=0.3 if k % 2 else 0.0) for k, n in enumerate(EDGE_SIZES)]
     kws = [params_dict(g, Physics((0.02, 0.05)[k % 2], (0.5, 0.7)[k % 3 == 0], 0.005, gas_drag=0.25,

@@ -10,7 +10,7 @@ import pytest
 
 from galaxy_sim_b200 import _lib
 from galaxy_sim_b200 import initial_conditions as ic
-from galaxy_sim_b200.autotune import autotune, get, set_
+from galaxy_sim_b200.autotune import autotune, get, launch_setting, set_
 from galaxy_sim_b200.nbody_gpu import NBodyGPU
 from galaxy_sim_b200.pool import GalaxyPool
 from galaxy_sim_b200.simulation import Physics, params_dict
@@ -35,7 +35,7 @@ def test_knobs_do_not_change_results(gpu_lib):
     g = ic.galaxy_disk(20000, 5, Q=1.2, arms=4, gas_frac=0.3)
     ph = Physics(0.02, 0.5, 0.005, gas_drag=0.25, sf_eff=0.02)
     P0, S0, e0 = _run(g, ph, None, None)
-    for bps, items in ((1, 8), (4, 16), (8, 8)):
+    for bps, items in ((1, 8), (4, 16), (8, 8), (7, 4)):
         P, S, e = _run(g, ph, bps, items)
         assert np.array_equal(P.view(np.uint32), P0.view(np.uint32)), (bps, items)
         assert np.array_equal(S.view(np.uint32), S0.view(np.uint32)), (bps, items)
@@ -165,10 +165,32 @@ def test_autotune_single_galaxy_tunes_the_split(gpu_lib):
     g = ic.galaxy_disk(16384, 21)
     sim = NBodyGPU(0, g.particles, g.stellar)
     sim.updateParams(dt=0.005, G=1.0, epsilon=0.05, theta=0.5)
-    res = autotune(sim, steps=2, warmup=1, walk_blocks=(7,), sort_items=(16,))
+    res = autotune(sim, steps=2, warmup=1, walk_groups=(0, 8), walk_blocks=(7,), sort_items=(16,))
     ch = res["choice"]
-    assert len(res["ms"]) == 11 and all(t > 0 for t in res["ms"].values())
+    assert len(res["ms"]) == 8 and all(t > 0 for t in res["ms"].values())
     assert get(sim._ctx, _lib.TUNE_WALK_SPLIT) == (0 if ch["walk_split"] == "by galaxy size" else ch["walk_split"])
+    eff = launch_setting(sim._ctx)
+    assert eff["walk_group"] == 8 and eff["sort_keys_per_thread"] == 16
+    assert eff["walk_split"] == (2 if ch["walk_split"] == "by galaxy size" else ch["walk_split"])
     sim.run(2, False)
     assert sim.deviceErrors() == 0
     sim.destroy()
+
+
+def test_launch_setting_follows_the_size_rules(gpu_lib):
+    """The by-size rules of a single-galaxy context, as the library applies them."""
+    for n, want in ((4096, (8, 4, 4)), (16384, (8, 2, 4)), (60000, (16, 1, 4)), (200000, (32, 1, 8)),
+                    (600000, (32, 1, 16))):
+        g = ic.galaxy_disk(n, 30)
+        sim = NBodyGPU(0, g.particles, g.stellar)
+        eff = launch_setting(sim._ctx)
+        assert (eff["walk_group"], eff["walk_split"], eff["sort_keys_per_thread"]) == want, (n, eff)
+        set_(sim._ctx, _lib.TUNE_WALK_GROUP, 32)
+        set_(sim._ctx, _lib.TUNE_WALK_SPLIT, 4)      # groups of 32 walk unsplit
+        assert launch_setting(sim._ctx)["walk_split"] == 1
+        sim.destroy()
+    pool = GalaxyPool(20000, 2)
+    pool._sel(pool.add(ic.galaxy_disk(3000, 31).particles))
+    eff = launch_setting(pool._ctx)
+    assert eff == {"walk_group": 32, "walk_split": 1, "sort_keys_per_thread": 16}, eff
+    pool.close()
