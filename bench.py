@@ -17,8 +17,9 @@ the context's stream, with a 256 MiB L2 flush (2x the 126 MB L2) between steps;
 barrier + synchronize on both sides; max over ranks. ``e2e`` is the same
 metric through the C ABI with pinned host buffers, frame by frame as main.js
 drives NBodyGPU at one step per frame: upload of the initial state, per step a
-Params upload, the step, the energy-diagnostic readback and the position
-readback (16 B per particle), and a final state readback, all inside the
+Params upload, the step and the position readback (16 B per particle, with the
+energy diagnostics of the same point) collected in the next frame as main.js
+collects its readback promise, and a final state readback, all inside the
 event-timed region. ``precision_modes`` gives the step time of the compensated
 walk and of the FP64 internal-node COM refresh on the same workload.
 
@@ -339,11 +340,12 @@ def run_ours(args, ws, rank, local):
         hs = torch.from_numpy(g.stellar.reshape(-1)).pin_memory()
         outp = torch.empty(N * 8, dtype=torch.float32).pin_memory()
         outs = torch.empty(N * 4, dtype=torch.float32).pin_memory()
-        outpos = torch.empty(N * 4, dtype=torch.float32).pin_memory()
+        # two frame buffers: a frame's positions stay readable while the next lands
+        outpos = [torch.empty(N * 4, dtype=torch.float32).pin_memory() for _ in range(2)]
         pd = params_dict(g, w.physics)
         sim.gpu.updateParams(**pd)
         prm = sim.gpu._params
-        diag = _lib.GsDiag()
+        diags = [_lib.GsDiag(), _lib.GsDiag()]
         ctx = sim.gpu._ctx
         Ke = K
         sim.sync()
@@ -356,25 +358,34 @@ def run_ours(args, ws, rank, local):
         _lib.check(L.gs_write_state(ctx, hp.data_ptr(), hs.data_ptr()), ctx)
         for k in range(Ke):
             # one frame of main.js:400-507 at one step per frame: Params with the
-            # clock, the step (rebuild on the device), the HUD's energy and the
-            # frame's position readback (vec4 pos + e_i per particle)
+            # clock, the step (rebuild on the device), then the frame's position
+            # readback (vec4 pos + e_i per particle) with the energy diagnostics of
+            # the same point. As in main.js:485-501 the readback resolves while the
+            # next frame's step runs, and one is in flight at a time: a frame
+            # collects the previous frame's before encoding its own.
             prm.time = k * w.physics.dt
             _lib.check(L.gs_update_params(ctx, C.byref(prm)), ctx)
             _lib.check(L.gs_run(ctx, 1, int(sim.star_formation)), ctx)
-            _lib.check(L.gs_energy(ctx, C.byref(diag)), ctx)
-            _lib.check(L.gs_read_positions(ctx, outpos.data_ptr(), 0), ctx)
+            if k:
+                _lib.check(L.gs_await_position_readback(ctx, 0), ctx)
+            _lib.check(L.gs_encode_position_readback(ctx, outpos[k % 2].data_ptr(),
+                                                     C.byref(diags[k % 2])), ctx)
+        _lib.check(L.gs_await_position_readback(ctx, 0), ctx)
+        diag = diags[(Ke - 1) % 2]
         _lib.check(L.gs_read_state(ctx, outp.data_ptr(), outs.data_ptr()), ctx)
         with torch.cuda.stream(ext):
             e1.record(ext)
         torch.cuda.synchronize()
         te_ms = rank_max(dist, e0.elapsed_time(e1), f"cuda:{local}")
-        if not np.isfinite(diag.e_diag) or not bool(torch.isfinite(outpos).all()):
+        if not np.isfinite(diag.e_diag) or not all(bool(torch.isfinite(b).all()) for b in outpos):
             raise RuntimeError("non-finite energy or positions in the e2e run")
         e2e = {"value": round(job_value(N * Ke, ws, te_ms), 1), "unit": UNIT,
                "h2d_bytes_per_step": int(round((N * 48 + Ke * 96) / Ke)),
                "d2h_bytes_per_step": int(round((Ke * (48 + 16 * N) + N * 48) / Ke)),
-               "path": "gs_write_state (pinned) + K frames of [gs_update_params, gs_run(1), gs_energy, "
-                       "gs_read_positions (pinned, 16 B/particle)] + gs_read_state (pinned)",
+               "path": "gs_write_state (pinned) + K frames of [gs_update_params, gs_run(1), "
+                       "gs_encode_position_readback (pinned, 16 B/particle + the energy diagnostics; "
+                       "awaited in the next frame, as main.js keeps one readback in flight)] + "
+                       "gs_read_state (pinned)",
                "steps": Ke, "ms": round(te_ms, 3)}
 
     # ---- config 0 (the 16384-particle disk): step and walk time per walk group size ----

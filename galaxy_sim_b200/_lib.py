@@ -74,6 +74,8 @@ SIGNATURES = [
     ("gs_step", _int, [_vp]),
     ("gs_star_formation", _int, [_vp]),
     ("gs_read_positions", _int, [_vp, _vp, C.c_uint64]),
+    ("gs_encode_position_readback", _int, [_vp, _vp, _vp]),
+    ("gs_await_position_readback", _int, [_vp, C.c_uint64]),
     ("gs_position_buffer", _int, [_vp, _vp]),
     ("gs_stellar_buffer", _int, [_vp, _vp]),
     ("gs_set_tracking", _int, [_vp, _i64, _i64, _vp, _vp]),

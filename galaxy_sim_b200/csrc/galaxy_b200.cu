@@ -244,6 +244,17 @@ struct gs_ctx {
   uint32_t walk_items[4] = {0, 0, 0, 0};  // work items per lanes-per-particle class (1, 2, 4, 8)
   bool walk_comp = false;  // Kahan-compensated far-field sums in the walk
   void* host_stage = nullptr;  // pinned: [slots] params
+  // asynchronous position readback (gs_encode_position_readback), set up on first
+  // use: a copy stream, the events ordering it after the compaction, a mapped
+  // pinned word block for the diagnostics snapshot and the error word, and the
+  // request in flight (at most one per context, like the reference's readbackInFlight)
+  cudaStream_t rb_stream = nullptr;
+  cudaEvent_t rb_ready = nullptr, rb_done = nullptr;
+  double* rb_host = nullptr;       // [kPartials] diagnostics, then the error word
+  double* rb_host_dev = nullptr;   // the same block as the device sees it
+  gs_diag* rb_diag = nullptr;      // caller's diagnostics destination (may be NULL)
+  uint32_t rb_slot = 0;
+  bool rb_pending = false;
   std::map<int, cudaGraphExec_t> graphs;
   uint32_t step_kernels = 0;  // kernel nodes of the last captured step graph
   char err[512] = "";
@@ -393,9 +404,18 @@ int pool_init(gs_ctx* c, int device, uint64_t cap, uint32_t slots) {
 void pool_release(gs_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->rb_stream) cudaStreamSynchronize(c->rb_stream);  // a readback in flight lands first
   c->drop_graphs();
   for (void* q : c->owned) cudaFree(q);
   c->owned.clear();
+  if (c->rb_host) cudaFreeHost(c->rb_host);
+  if (c->rb_ready) cudaEventDestroy(c->rb_ready);
+  if (c->rb_done) cudaEventDestroy(c->rb_done);
+  if (c->rb_stream) cudaStreamDestroy(c->rb_stream);
+  c->rb_host = c->rb_host_dev = nullptr;
+  c->rb_ready = c->rb_done = nullptr;
+  c->rb_stream = nullptr;
+  c->rb_pending = false;
   if (c->host_stage) cudaFreeHost(c->host_stage);
   if (c->ev) cudaEventDestroy(c->ev);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -1204,12 +1224,85 @@ int gs_read_positions(gs_ctx* ctx, float* out4, uint64_t timeout_ns) {
   CTX_CHECK(ctx);
   SLOT(ctx, s);
   if (!out4) return ctx->fail(GS_EINVAL, "out4 is NULL");
+  // an asynchronous readback still copying out of the compaction buffer finishes first
+  if (ctx->rb_pending) CK(ctx, cudaStreamWaitEvent(ctx->stream, ctx->rb_done, 0), "readback order");
   compact_kernel<<<grid_for(s->n, 256, 148 * 16), 256, 0, ctx->stream>>>(
       ctx->part[ctx->cur] + 2 * (size_t)s->off, ctx->energy + s->off, ctx->compact + s->off, s->n);
   CK(ctx, cudaGetLastError(), "compact");
   int rc = wait_stream(ctx, timeout_ns, s);
   if (rc) return rc;
   CK(ctx, cudaMemcpy(out4, ctx->compact + s->off, (size_t)s->n * 16, cudaMemcpyDeviceToHost), "readback");
+  return GS_OK;
+}
+
+int gs_encode_position_readback(gs_ctx* ctx, float* out4, gs_diag* diag) {
+  CTX_CHECK(ctx);
+  SLOT(ctx, s);
+  if (!out4) return ctx->fail(GS_EINVAL, "out4 is NULL");
+  if (ctx->rb_pending)
+    return ctx->fail(GS_ENOTREADY, "a position readback is in flight: await it before encoding another");
+  if (!ctx->rb_stream) {  // first use: copy stream, events, mapped pinned words
+    CK(ctx, cudaStreamCreateWithFlags(&ctx->rb_stream, cudaStreamNonBlocking), "readback stream");
+    CK(ctx, cudaEventCreateWithFlags(&ctx->rb_ready, cudaEventDisableTiming), "readback event");
+    CK(ctx, cudaEventCreateWithFlags(&ctx->rb_done, cudaEventDisableTiming), "readback event");
+    void* h = nullptr;
+    CK(ctx, cudaHostAlloc(&h, (kPartials + 1) * sizeof(double), cudaHostAllocMapped), "readback words");
+    ctx->rb_host = static_cast<double*>(h);
+    void* d = nullptr;
+    CK(ctx, cudaHostGetDevicePointer(&d, h, 0), "readback words");
+    ctx->rb_host_dev = static_cast<double*>(d);
+  }
+  // in stream order: vec4(pos, e_i) into the compaction buffer and the diagnostics
+  // snapshot; the copy stream then moves the positions while later steps run
+  compact_kernel<<<grid_for(s->n, 256, 148 * 16), 256, 0, ctx->stream>>>(
+      ctx->part[ctx->cur] + 2 * (size_t)s->off, ctx->energy + s->off, ctx->compact + s->off, s->n);
+  CK(ctx, cudaGetLastError(), "compact");
+  readback_snapshot_kernel<<<1, 32, 0, ctx->stream>>>(ctx->diag_out + (size_t)ctx->sel * kPartials,
+                                                      &ctx->st[ctx->sel].err, ctx->rb_host_dev);
+  CK(ctx, cudaGetLastError(), "readback snapshot");
+  CK(ctx, cudaEventRecord(ctx->rb_ready, ctx->stream), "readback event");
+  CK(ctx, cudaStreamWaitEvent(ctx->rb_stream, ctx->rb_ready, 0), "readback order");
+  CK(ctx, cudaMemcpyAsync(out4, ctx->compact + s->off, (size_t)s->n * 16, cudaMemcpyDeviceToHost, ctx->rb_stream),
+     "readback copy");
+  CK(ctx, cudaEventRecord(ctx->rb_done, ctx->rb_stream), "readback event");
+  ctx->rb_diag = diag;
+  ctx->rb_slot = ctx->sel;
+  ctx->rb_pending = true;
+  return GS_OK;
+}
+
+int gs_await_position_readback(gs_ctx* ctx, uint64_t timeout_ns) {
+  CTX_CHECK(ctx);
+  if (!ctx->rb_pending) return ctx->fail(GS_EINVAL, "no position readback in flight");
+  if (timeout_ns == 0) {
+    CK(ctx, cudaEventSynchronize(ctx->rb_done), "readback wait");
+  } else {
+    const auto t0 = std::chrono::steady_clock::now();
+    while (true) {
+      cudaError_t q = cudaEventQuery(ctx->rb_done);
+      if (q == cudaSuccess) break;
+      if (q != cudaErrorNotReady) return ctx->cuda(q, "readback wait");
+      const auto dt =
+          std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count();
+      if ((uint64_t)dt > timeout_ns)  // still in flight: a later await can collect it
+        return ctx->fail(GS_ETIMEDOUT, "position readback did not land within %llu ns",
+                         (unsigned long long)timeout_ns);
+      std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+  }
+  ctx->rb_pending = false;
+  if (ctx->rb_diag) {
+    const double* h = ctx->rb_host;
+    ctx->rb_diag->e_diag = h[0];
+    ctx->rb_diag->e_true = h[1];
+    ctx->rb_diag->momentum[0] = h[2];
+    ctx->rb_diag->momentum[1] = h[3];
+    ctx->rb_diag->momentum[2] = h[4];
+    ctx->rb_diag->mass = h[5];
+  }
+  const unsigned err = reinterpret_cast<const unsigned*>(ctx->rb_host + kPartials)[0];
+  if (err)
+    return ctx->fail(GS_EDEVICE, "device error word 0x%x of slot %u at the readback", err, ctx->rb_slot);
   return GS_OK;
 }
 

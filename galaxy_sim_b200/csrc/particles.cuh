@@ -287,6 +287,16 @@ __global__ void compact_kernel(const float4* __restrict__ P, const float* __rest
   }
 }
 
+// Snapshot of one galaxy's diagnostics (kPartials doubles) and error word into
+// mapped pinned host memory, in stream order: the asynchronous readback delivers
+// the values of the step it follows even when later steps overwrite them.
+__global__ void readback_snapshot_kernel(const double* __restrict__ diag, const unsigned* __restrict__ err,
+                                         double* host) {
+  const int t = threadIdx.x;
+  if (t < kPartials) host[t] = diag[t];
+  if (t == kPartials) reinterpret_cast<unsigned*>(host + kPartials)[0] = *err;
+}
+
 // refresh_level (nbody_bh.wgsl:288-313) on one BFS level of the walk layout
 // (pool indices).
 __global__ void refresh_level_kernel(const float4* __restrict__ P, float4* cm,

@@ -184,7 +184,9 @@ __device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k
                                          float2& pt, float& selfw, unsigned long long& npair,
                                          bool dbg, uint32_t sub) {
   if (soft) {
-    const float2 wme = make_float2(me ? 1.0f : 0.0f, me ? 1.0f : 0.0f);
+    // a lane that did not open the leaf gets eps^2 = +inf: its r^2 + eps^2 is
+    // +inf, rsqrt gives 0 and every term of the pair vanishes (r is finite)
+    const float e2me = me ? eps2 : INFINITY;
     if (me && jself < k && ((jself >> 1) % LPP) == sub) selfw += 1.0f;
     for (uint32_t j = 2 * sub; j < kmax; j += 2 * LPP) {
       const float4 jxy = *reinterpret_cast<const float4*>(&S.lxy[2 * (off + j)]);
@@ -192,8 +194,8 @@ __device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k
       const float2 jx = make_float2(jxy.x, jxy.y), jy = make_float2(jxy.z, jxy.w);
       const float2 jz = make_float2(jzm.x, jzm.y), jm = make_float2(jzm.z, jzm.w);
       const float2 ex = __fadd2_rn(jx, px), ey = __fadd2_rn(jy, py), ez = __fadd2_rn(jz, pz);
-      const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __ffma2_rn(ez, ez, make_float2(eps2, eps2))));
-      const float2 ri = __fmul2_rn(make_float2(rsqrtf(e2.x), rsqrtf(e2.y)), wme);
+      const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __ffma2_rn(ez, ez, make_float2(e2me, e2me))));
+      const float2 ri = make_float2(rsqrtf(e2.x), rsqrtf(e2.y));
       const float2 mr = __fmul2_rn(jm, ri);
       const float2 ff = __fmul2_rn(__fmul2_rn(mr, ri), ri);
       ax = __ffma2_rn(ex, ff, ax);
@@ -235,18 +237,10 @@ __device__ __forceinline__ void kahan_add2(float2& s, float2& c, float2 x) {
   s = t;
 }
 
-// 1.0f if a > b else 0.0f (ordered compare: NaN gives 0), as one compare-and-set.
-__device__ inline float set_gt(float a, float b) {
-  float r;
-  asm("set.gt.f32.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
-  return r;
-}
-
-// All ones if !(a > b) (a <= b or unordered), else 0, as one compare-and-set:
-// the open bit of a node whose weight set_gt(a, b) is 0.
-__device__ inline uint32_t set_leu(float a, float b) {
+// All ones if a > b (ordered: NaN gives 0), else 0, as one compare-and-set.
+__device__ inline uint32_t set_gt_mask(float a, float b) {
   uint32_t r;
-  asm("set.leu.u32.f32 %0, %1, %2;" : "=r"(r) : "f"(a), "f"(b));
+  asm("set.gt.u32.f32 %0, %1, %2;" : "=r"(r) : "f"(a), "f"(b));
   return r;
 }
 
@@ -362,14 +356,9 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
       const int nr = min(sp, kWalkRanges);
       const int sp0 = sp;
       sp -= nr;
-      uint32_t masks[kWalkRanges];
-      uint32_t cnts = 0;  // 4 bits per range
+      uint32_t masks[kWalkRanges];  // lanes that opened each popped range's parent
 #pragma unroll
-      for (int r = 0; r < kWalkRanges; r++) {
-        const uint2 e = r < nr ? S.stack[sp0 - 1 - r] : make_uint2(0u, 0u);
-        masks[r] = e.y;
-        cnts |= (r < nr ? (e.x >> 29) + 1u : 0u) << (4 * r);
-      }
+      for (int r = 0; r < kWalkRanges; r++) masks[r] = r < nr ? S.stack[sp0 - 1 - r].y : 0u;
       if (--budget == 0) {
         if (lane == 0) raise_err(sst, GS_DERR_STACK);
         break;
@@ -428,13 +417,15 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
       const unsigned massmask = DBG ? __ballot_sync(full, massive) : 0u;
       const unsigned skipm = NS > 1 ? __ballot_sync(full, skip) : 0u;  // opened leaves another split sums
       __syncwarp();
-      uint32_t actbits = 0, keep = 0;  // per range: this lane active; slots this lane may open
+      // per range: this lane active; the slots whose open bits this lane keeps (its
+      // active ranges' eight slots: a slot past a range's count holds a dummy of
+      // size^2 -inf, which every active lane accepts, so it never sets an open bit)
+      uint32_t actbits = 0, keep = 0;
 #pragma unroll
       for (int r = 0; r < kWalkRanges; r++) {
         const uint32_t a_r = (masks[r] >> pl) & 1u;
         actbits |= a_r << r;
-        const uint32_t cr = (cnts >> (4 * r)) & 15u;
-        keep |= a_r ? ((1u << cr) - 1u) << (8 * r) : 0u;
+        keep |= a_r ? 0xffu << (8 * r) : 0u;
       }
       keep &= mine;
       // theta^2 per range; a lane inactive for a range tests against -inf, so its
@@ -442,10 +433,11 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
       float th2[kWalkRanges];
 #pragma unroll
       for (int r = 0; r < kWalkRanges; r++) th2[r] = (actbits >> r) & 1u ? theta2 : -INFINITY;
-      uint32_t obits = 0;  // children this lane opens (active, accept weight 0), bit = slot
+      uint32_t obits = 0;  // children this lane opens (active, not accepted), bit = slot
 #pragma unroll
       for (int kk = 0; kk < NPP; kk++) {
-        if (kk * LPP >= 4 * nr) break;
+        // a range's pairs are tested only if the range was popped (one check per range)
+        if ((kk * LPP) % 4 == 0 && kk * LPP >= 4 * nr) break;
         const int pp = (int)sub + kk * LPP;
         const int c = 2 * pp;
         // the pair's range pp >> 2: (kk * LPP) >> 2 for shares below 4, one more above
@@ -458,9 +450,13 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
         const float2 rx = __fadd2_rn(qx, px), ry = __fadd2_rn(qy, py), rz = __fadd2_rn(qz, pz);
         const float2 d2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __ffma2_rn(rz, rz, f2(eps2))));
         const float2 td = __fmul2_rn(f2(t2), d2);
-        const float2 w = make_float2(set_gt(td.x, s2.x), set_gt(td.y, s2.y));
-        obits |= (set_leu(td.x, s2.x) & (1u << c)) | (set_leu(td.y, s2.y) & (2u << c));  // w == 0
-        const float2 rinv = __fmul2_rn(make_float2(rsqrtf(d2.x), rsqrtf(d2.y)), w);
+        // all ones where the child is accepted; an accepted child keeps r^2 + eps^2,
+        // any other gets +inf, so rsqrt makes its terms exactly 0
+        const uint32_t ax_ = set_gt_mask(td.x, s2.x), ay_ = set_gt_mask(td.y, s2.y);
+        obits |= (~ax_ & (1u << c)) | (~ay_ & (2u << c));
+        const float2 dsel = make_float2(__uint_as_float((__float_as_uint(d2.x) & ax_) | (0x7f800000u & ~ax_)),
+                                        __uint_as_float((__float_as_uint(d2.y) & ay_) | (0x7f800000u & ~ay_)));
+        const float2 rinv = make_float2(rsqrtf(dsel.x), rsqrtf(dsel.y));
         const float2 mr = __fmul2_rn(qm, rinv);
         const float2 f = __fmul2_rn(__fmul2_rn(mr, rinv), rinv);
         if (COMP) {

@@ -128,18 +128,47 @@ class NBodyGPU:
             return
         self._ok(lib().gs_step(self._ctx))
 
-    def encodePositionReadback(self, commandEncoder=None):
-        """The compaction is done inside readPositions (one stream, same ordering)."""
+    def encodePositionReadback(self, commandEncoder=None, staging=None):
+        """NBodyGPU.js:334-341: queue the compaction of vec4(pos, e_i) and its copy to
+        host memory behind the work already queued, without waiting (a readback
+        already in flight raises GalaxyError GS_ENOTREADY, like the reference's
+        one-map rule); readPositions collects it. ``staging`` (N*4 contiguous
+        float32, pinned for the copy to overlap later steps) is where it lands; by
+        default a buffer of this object. The galaxy's energy diagnostics of the same
+        point arrive with it (``readbackEnergy`` after readPositions)."""
+        if not self.ready:
+            return None
+        if staging is None:
+            if getattr(self, "_staging", None) is None:
+                self._staging = np.zeros(4 * self.N, np.float32)
+            staging = self._staging
+        buf = np.asarray(staging).reshape(-1)
+        if buf.dtype != np.float32 or buf.size < 4 * self.N or not buf.flags.c_contiguous:
+            raise ValueError("staging must be contiguous float32 with N*4 elements")
+        diag = GsDiag()
+        self._ok(lib().gs_encode_position_readback(self._ctx, ptr(buf), C.byref(diag)))
+        self._rb = (buf, diag)  # both must outlive the copy
         return None
 
     def readPositions(self, out=None, timeout_ns=0):
-        """NBodyGPU.js:346-350: vec4(pos, e_i) per particle."""
-        buf = np.zeros(4 * self.N, np.float32)
-        self._ok(lib().gs_read_positions(self._ctx, ptr(buf), int(timeout_ns)))
+        """NBodyGPU.js:344-348: vec4(pos, e_i) per particle. Awaits the readback
+        encodePositionReadback queued (at most timeout_ns, 0 = no limit; a timeout
+        raises and leaves it in flight), or reads the current state when none is."""
+        rb = getattr(self, "_rb", None)
+        if rb is not None:
+            self._ok(lib().gs_await_position_readback(self._ctx, int(timeout_ns)))
+            self._rb = None
+            buf, d = rb
+            self.readbackEnergy = {"e_diag": d.e_diag, "e_true": d.e_true,
+                                   "momentum": list(d.momentum), "mass": d.mass}
+            buf = buf[: 4 * self.N]
+        else:
+            buf = np.zeros(4 * self.N, np.float32)
+            self._ok(lib().gs_read_positions(self._ctx, ptr(buf), int(timeout_ns)))
         if out is not None:
             np.asarray(out).reshape(-1)[: buf.size] = buf
             return out
-        return buf
+        return buf.copy() if rb is not None else buf
 
     @property
     def positionBuffer(self) -> int:

@@ -169,6 +169,22 @@ int gs_star_formation(gs_ctx* ctx);
 /* encodePositionReadback + readPositions (NBodyGPU.js:335-350): vec4(pos, e_i)
  * per particle into out4 (N*4 floats); waits at most timeout_ns (0 = no limit). */
 int gs_read_positions(gs_ctx* ctx, float* out4, uint64_t timeout_ns);
+/* The same readback without waiting, as the reference drives it: encodePositionReadback
+ * (NBodyGPU.js:334-341) queues the compaction and copy behind the work already
+ * queued, and the promise of readPositions (NBodyGPU.js:344-348) resolves later while
+ * main.js:485-501 keeps stepping with at most one readback in flight.
+ * gs_encode_position_readback queues vec4(pos, e_i) of the selected galaxy into out4
+ * (N*4 floats) and, if diag is not NULL, that galaxy's energy/momentum diagnostics as
+ * of the same point, then returns. The copy runs on a second stream: with out4 in
+ * pinned host memory it overlaps the steps queued after it (pageable memory works but
+ * the call then returns only when the copy is done). out4 and diag must stay valid
+ * until gs_await_position_readback returns GS_OK. A second encode while one is in
+ * flight returns GS_ENOTREADY. The first call sets up the copy stream and a small
+ * pinned block. gs_await_position_readback waits at most timeout_ns (0 = no limit;
+ * GS_ETIMEDOUT leaves the readback in flight), fills diag and returns GS_EDEVICE if
+ * the galaxy's device error word was set at that point. */
+int gs_encode_position_readback(gs_ctx* ctx, float* out4, gs_diag* diag);
+int gs_await_position_readback(gs_ctx* ctx, uint64_t timeout_ns);
 /* positionBuffer / stellarBuffer getters (NBodyGPU.js:241-243, :353-356):
  * device pointers of the current buffers (valid until the next flip). */
 int gs_position_buffer(gs_ctx* ctx, void** dptr);

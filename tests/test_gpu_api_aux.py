@@ -11,6 +11,9 @@
   that FP32 and FP64 decide differently; reset returns and clears them.
 * gs_sync waits for queued work, bounded by a timeout; a wait that times out
   leaves the queued work and the context intact.
+* The asynchronous position readback (gs_encode_position_readback /
+  gs_await_position_readback) delivers the state of the step it followed while
+  later steps run, one readback in flight at a time, with a bounded await.
 """
 import numpy as np
 import pytest
@@ -109,4 +112,81 @@ def test_sync_timeout_leaves_the_context_usable(gpu_lib):
     sim.sync(timeout_ns=60_000_000_000)
     P, _ = sim.readState()
     assert np.all(np.isfinite(P)) and sim.deviceErrors() == 0
+    sim.destroy()
+
+
+def test_async_position_readback_follows_its_step(gpu_lib):
+    """gs_encode_position_readback / gs_await_position_readback, driven as
+    main.js:485-501 drives encodePositionReadback and the readPositions promise
+    (NBodyGPU.js:334-348): each frame queues its step, collects the previous
+    frame's readback and encodes its own, so a readback is collected after the
+    next step was queued. Every readback holds vec4(pos, e_i) and the energy
+    diagnostics of the step it followed: the synchronous readback and gs_energy
+    of a second context stepped in lock step, bit for bit. One readback is in
+    flight at a time (a second encode returns GS_ENOTREADY, leaving the first
+    intact); an await with nothing in flight is GS_EINVAL."""
+    import ctypes as C
+
+    import torch
+
+    g = ic.disk_16k()
+    kw = dict(dt=0.005, G=1.0, epsilon=0.05, theta=0.5)
+    a, b = NBodyGPU(0, g.particles, g.stellar), NBodyGPU(0, g.particles, g.stellar)
+    a.updateParams(**kw)
+    b.updateParams(**kw)
+    L = _lib.lib()
+    bufs = [torch.empty(4 * g.N, dtype=torch.float32).pin_memory() for _ in range(2)]
+    diags = [_lib.GsDiag(), _lib.GsDiag()]
+    assert L.gs_await_position_readback(a._ctx, 0) == _lib.GS_EINVAL
+    got, want = [], []
+
+    def collect(k):
+        _lib.check(L.gs_await_position_readback(a._ctx, 0), a._ctx)
+        d = diags[k % 2]
+        got.append((bufs[k % 2].numpy().copy(), (d.e_diag, d.e_true, *d.momentum, d.mass)))
+
+    for k in range(4):
+        a.run(1, False)
+        if k:
+            collect(k - 1)
+        _lib.check(L.gs_encode_position_readback(a._ctx, bufs[k % 2].data_ptr(), C.byref(diags[k % 2])),
+                   a._ctx)
+        assert L.gs_encode_position_readback(a._ctx, bufs[(k + 1) % 2].data_ptr(), None) == _lib.GS_ENOTREADY
+        b.run(1, False)
+        e = b.energy()
+        want.append((b.readPositions(), (e["e_diag"], e["e_true"], *e["momentum"], e["mass"])))
+    collect(3)
+    for (gp, gd), (wp, wd) in zip(got, want):
+        assert _same(gp, wp)
+        assert gd == wd
+    assert a.deviceErrors() == 0
+    a.destroy()
+    b.destroy()
+
+
+def test_async_position_readback_timeout_and_python_mirror(gpu_lib):
+    """A bounded await that expires returns GS_ETIMEDOUT and leaves the readback in
+    flight; a later await collects it. The Python mirror's encodePositionReadback
+    + readPositions return the positions of the point the readback was encoded at,
+    even with more steps queued after it."""
+    import torch
+
+    g = ic.disk_16k()
+    sim = NBodyGPU(0, g.particles, g.stellar)
+    sim.updateParams(dt=0.005, G=1.0, epsilon=0.05, theta=0.5)
+    # pinned: a copy into pageable memory returns only once it is done
+    staging = torch.empty(4 * g.N, dtype=torch.float32).pin_memory().numpy()
+    sim.run(1000, False)                       # a few hundred ms of queued steps
+    sim.encodePositionReadback(staging=staging)
+    with pytest.raises(_lib.GalaxyError) as e:
+        sim.readPositions(timeout_ns=1)
+    assert e.value.code == _lib.GS_ETIMEDOUT
+    late = sim.readPositions(timeout_ns=60_000_000_000)
+    assert _same(late, sim.readPositions())    # nothing queued since: the same state
+    sim.encodePositionReadback()
+    sim.run(3, False)
+    before = sim.readPositions()
+    after = sim.readPositions()
+    assert not _same(before, after) and np.all(np.isfinite(before))
+    assert sim.readbackEnergy["mass"] > 0 and sim.deviceErrors() == 0
     sim.destroy()
