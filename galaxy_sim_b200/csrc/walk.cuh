@@ -166,17 +166,17 @@ struct WalkSmem {
   // staged leaf sources, pair-interleaved the same way (pairs 0..32)
   __align__(16) float lxy[136];
   __align__(16) float lzm[136];
-  uint4 bl[8 * kWalkRanges];        // opened small leaves: {first particle, count, lane mask, 0}
+  uint4 bl[32];  // a round's opened leaves: {first particle, count, opening mask, first pair}
 };
 
 // Direct sum of a staged leaf segment [off, off + k) for the lanes in `me`
-// (nbody_bh.wgsl:117-131), two sources per packed step, up to kmax >= k (staged
-// sources past a leaf's count are massless zeros). A particle served by LPP
-// lanes splits the source pairs: lane
-// `sub` takes pairs sub, sub + LPP, ... With soft (eps^2 > 0) the self pair is
-// included (zero force at r = 0) and its potential removed once at the end of
-// the walk via selfw (counted by the lane whose share holds it); otherwise it is
-// skipped per pair.
+// (nbody_bh.wgsl:117-131), used by walk groups of 32: two sources per packed
+// step, up to kmax >= k (staged sources past a leaf's count are massless zeros).
+// A particle served by LPP lanes splits the source pairs: lane `sub` takes pairs
+// sub, sub + LPP, ... With soft (eps^2 > 0) the self pair is included (zero
+// force at r = 0) and its potential removed once at the end of the walk via
+// selfw (counted by the lane whose share holds it); otherwise it is skipped per
+// pair.
 template <int LPP, typename Smem>
 __device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k, uint32_t kmax, uint32_t jself,
                                          bool me, bool soft, float2 px, float2 py, float2 pz,
@@ -223,6 +223,53 @@ __device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k
       pt = __fadd2_rn(pt, mr);
       if (dbg) npair += u0 + u1;
     }
+  }
+}
+
+// Direct sums of one staged batch of leaf sources for walk groups of 16 or fewer
+// (nbody_bh.wgsl:117-131): up to 32 source pairs, pair t pair-interleaved at
+// lxy/lzm[4t..4t+3], each pair from one leaf (a leaf of odd count ends in a
+// massless zero). A particle served by LPP lanes splits the pairs: lane `sub`
+// takes pairs sub, sub + LPP, ... Bit LPP * kk of `pm` tells whether the
+// particle opened the leaf of pair sub + LPP * kk.
+// With soft (eps^2 > 0) a pair the lane does not take gets eps^2 = +inf: r^2 +
+// eps^2 is then +inf, rsqrt gives 0 and every term vanishes (r is finite); the
+// self pair is included (zero force at r = 0) and its potential removed once at
+// the end of the walk. Without softening the self pair (batch source `selfloc`)
+// is skipped per pair. Pairs past nbp hold massless zeros and are never in pm.
+template <int LPP, bool SOFT, typename Smem>
+__device__ __forceinline__ void leaf_batch(const Smem& S, uint32_t nbp, uint32_t pm, uint32_t selfloc,
+                                           float2 px, float2 py, float2 pz, float eps2, float2& ax,
+                                           float2& ay, float2& az, float2& pt, uint32_t sub) {
+  constexpr int NB = 32 / LPP;  // steps of a lane over a full batch
+  const float* lx = &S.lxy[4 * sub];
+  const float* lz = &S.lzm[4 * sub];
+#pragma unroll
+  for (int kk = 0; kk < NB; kk++) {
+    if ((kk * LPP) % 4 == 0 && kk * LPP >= (int)nbp) break;  // one check per four pairs
+    const float4 jxy = *reinterpret_cast<const float4*>(lx + 4 * LPP * kk);
+    const float4 jzm = *reinterpret_cast<const float4*>(lz + 4 * LPP * kk);
+    const float2 jx = make_float2(jxy.x, jxy.y), jy = make_float2(jxy.z, jxy.w);
+    const float2 jz = make_float2(jzm.x, jzm.y), jm = make_float2(jzm.z, jzm.w);
+    const float2 ex = __fadd2_rn(jx, px), ey = __fadd2_rn(jy, py), ez = __fadd2_rn(jz, pz);
+    const bool me = (pm >> (LPP * kk)) & 1u;
+    float2 ri;
+    if (SOFT) {
+      const float e2me = me ? eps2 : INFINITY;
+      const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __ffma2_rn(ez, ez, make_float2(e2me, e2me))));
+      ri = make_float2(rsqrtf(e2.x), rsqrtf(e2.y));
+    } else {
+      const uint32_t j2 = 2 * (sub + LPP * kk);  // the pair's first source in the batch
+      const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __ffma2_rn(ez, ez, make_float2(eps2, eps2))));
+      ri = make_float2(me && j2 != selfloc ? rsqrtf(e2.x) : 0.0f,
+                       me && j2 + 1 != selfloc ? rsqrtf(e2.y) : 0.0f);
+    }
+    const float2 mr = __fmul2_rn(jm, ri);
+    const float2 ff = __fmul2_rn(__fmul2_rn(mr, ri), ri);
+    ax = __ffma2_rn(ex, ff, ax);
+    ay = __ffma2_rn(ey, ff, ay);
+    az = __ffma2_rn(ez, ff, az);
+    pt = __fadd2_rn(pt, mr);
   }
 }
 
@@ -515,12 +562,13 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
         if (sp + np > kWalkStack && lane == 0) raise_err(sst, GS_DERR_STACK);  // not for depth <= 10 trees
         sp = min(sp + np, kWalkStack);
       }
-      // opened leaves: direct sums, two sources at a time. Leaves of <= 16
-      // particles get their batch entries from their slots' lanes and are staged
-      // four per batch (one load round); larger ones go in chunks of 32.
+      // Opened leaves: direct sums, two sources at a time.
       const uint32_t leafc = om & leafmask & ~skipm;
+      // Walk groups of 32: leaves of <= 16 particles get their batch entries from
+      // their slots' lanes and are staged four per batch (one load round), each in
+      // a block of 16 sources; larger ones go in chunks of 32.
       uint32_t big = 0;
-      if (leafc) {
+      if (LPP == 1 && leafc) {
         bool sm = false, bg = false;
         uint4 ent = make_uint4(0u, 0u, 0u, 0u);
         if ((leafc >> lane) & 1u) {
@@ -583,6 +631,97 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
           __syncwarp();
           leaf_sum<LPP>(S, 0, k, k, i - (cchild + b0), (open >> pl) & 1u, soft, px, py, pz, eps2, ax, ay,
                         az, pt, selfw, npair, DBG, sub);
+        }
+      }
+      // Walk groups of 16 or fewer (a particle's pairs split over LPP lanes): the
+      // round's opened leaves lie back to back in slot order in a space of source
+      // pairs (leaf k at pairs [P_k, P_k + ceil(n_k / 2))), staged and summed in
+      // batches of 32 pairs, so every lane's share of a batch is whole pairs of
+      // leaf sources and no step is spent on a leaf's unused staging slots.
+      if (LPP > 1 && leafc) {
+        bool lf = false;
+        uint32_t lfirst = 0, lcnt = 0, lnp = 0;
+        if ((leafc >> lane) & 1u) {
+          const uint4 mt = S.cmeta[lane];
+          lfirst = mt.x;
+          lcnt = mt.y & ~kLeafBit;
+          if ((uint64_t)lfirst + lcnt > a.pool_n) {
+            raise_err(sst, GS_DERR_TREE);
+          } else {
+            lf = lcnt > 0u;  // an empty leaf adds nothing
+            lnp = (lcnt + 1u) >> 1;
+          }
+        }
+        uint32_t incl = lnp;  // inclusive prefix of the pair counts over the slots
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(full, incl, o);
+          if (lane >= o) incl += y;
+        }
+        const uint32_t P = incl - lnp, T = __shfl_sync(full, incl, 31);
+        const uint32_t lfm = __ballot_sync(full, lf);
+        // item particles that opened the leaf holding them (the self pair)
+        uint32_t selfm = 0;
+        if (lf) {
+          const uint32_t lo = max(lfirst, gbeg), hi = min(lfirst + lcnt, gend);
+          if (lo < hi) {
+            const uint32_t b0 = lo - gbeg, b1 = hi - gbeg;  // item particle positions [b0, b1)
+            selfm = col & ((b1 >= 32u ? 0xffffffffu : (1u << b1) - 1u) & ~((1u << b0) - 1u));
+          }
+        }
+        const bool selfhit = (__reduce_or_sync(full, selfm) >> pl) & 1u;
+        if (soft && sub == 0 && selfhit) selfw += 1.0f;
+        __syncwarp();  // the previous round's batches are done reading the table and staging
+        if (lf) S.bl[__popc(lfm & ((1u << lane) - 1u))] = make_uint4(lfirst, lcnt, col, P);
+        __syncwarp();
+        uint32_t selfsrc = 0xffffffffu;  // without softening: the self source in pair space
+        if (DBG || !soft) {
+          const uint32_t nl = __popc(lfm);
+          for (uint32_t k = 0; k < nl; k++) {
+            const uint4 L = S.bl[k];
+            if ((L.z >> pl) & 1u) {
+              const bool in = i - L.x < L.y;
+              if (in) selfsrc = 2 * L.w + (i - L.x);
+              if (DBG && sub == 0) npair += L.y - (in ? 1u : 0u);
+            }
+          }
+        }
+        for (uint32_t w0 = 0; w0 < T; w0 += 32) {
+          // leaves starting in this batch's window of pairs, and those before it
+          const uint32_t Wb = __reduce_or_sync(full, lf && P >= w0 && P - w0 < 32u ? 1u << (P - w0) : 0u);
+          const uint32_t base = __popc(__ballot_sync(full, lf && P < w0));
+          if (w0) __syncwarp();  // the previous batch's sums are done reading the staging
+          // stage source e = lane + 32 r of the batch: pair t = e / 2 of leaf k
+#pragma unroll
+          for (int r = 0; r < 2; r++) {
+            const uint32_t e = lane + 32 * r, t = e >> 1;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (w0 + t < T) {
+              const uint4 L = S.bl[base + __popc(Wb & (0xffffffffu >> (31 - t))) - 1];
+              const uint32_t q = 2 * (w0 + t - L.w) + (e & 1u);  // source within the leaf
+              if (q < L.y) v = __ldg(&a.pin[2 * (size_t)(L.x + q)]);
+            }
+            const uint32_t se = 4 * t + (e & 1u);
+            S.lxy[se] = v.x;
+            S.lxy[se + 2] = v.y;
+            S.lzm[se] = v.z;
+            S.lzm[se + 2] = v.w;
+          }
+          // lane t answers for pair t: the item particles that opened its leaf
+          // (copied to every share when LPP > 1); transposed, each lane holds the
+          // pairs its particle takes part in
+          uint32_t mt = 0;
+          if (w0 + lane < T) mt = S.bl[base + __popc(Wb & (0xffffffffu >> (31 - lane))) - 1].z;
+          if (LPP == 2) mt *= 0x00010001u;
+          if (LPP == 4) mt *= 0x01010101u;
+          if (LPP == 8) mt *= 0x11111111u;
+          const uint32_t pm = warp_transpose(mt, lane) >> sub;
+          const uint32_t nbp = min(32u, T - w0);
+          __syncwarp();
+          if (soft)
+            leaf_batch<LPP, true>(S, nbp, pm, 0u, px, py, pz, eps2, ax, ay, az, pt, sub);
+          else
+            leaf_batch<LPP, false>(S, nbp, pm, selfsrc - 2 * w0, px, py, pz, eps2, ax, ay, az, pt, sub);
         }
       }
     }
