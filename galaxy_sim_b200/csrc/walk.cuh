@@ -18,7 +18,10 @@
 //     staging work is shared by up to 32 children.
 //   * Children are tested two at a time, and an opened leaf's particles are
 //     staged the same way and summed two at a time, with sm_100's packed
-//     FP32x2 FMA/ADD/MUL; accumulation is predicated, not branched.
+//     FP32x2 FMA/ADD/MUL; accumulation is predicated, not branched (a child or
+//     source a lane does not take gets r^2 + eps^2 = +inf, so rsqrt gives 0).
+//     Walk groups of 16 or fewer stage a round's opened leaves back to back and
+//     sum them in batches of 32 source pairs (see the leaf section).
 //   * Warps are persistent and take work items from an atomic counter (load
 //     balance across the dense core); per-item FP64 partials of the
 //     diagnostics replace a block-wide barrier.
