@@ -362,10 +362,15 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
     const uint32_t gbeg = sd.off + (gcur - sd.group0) * kWalkGroup + part * G, gend = gbeg + G;
     const uint32_t i = gbeg + pl;
     const bool valid = i < seg_end;
+    // Walk groups of 32 read the particle's record again for the integration at
+    // the end, so only its negated position stays live through the walk (the
+    // 64-register build then needs no spills; measured faster for pools, the
+    // same for one large galaxy); smaller groups keep it (measured faster there).
+    constexpr bool kReload = LPP == 1;
     float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0;
     if (valid) {
       p0 = a.pin[2 * (size_t)i];
-      p1 = a.pin[2 * (size_t)i + 1];
+      if (!kReload) p1 = a.pin[2 * (size_t)i + 1];
     }
     const float2 px = f2(-p0.x), py = f2(-p0.y), pz = f2(-p0.z);  // negated: r = q + (-p)
     float2 ax = f2(0.f), ay = f2(0.f), az = f2(0.f), pt = f2(0.f);
@@ -806,6 +811,10 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
         dens = u2.x;
         selfw = u2.y;
       }
+    }
+    if (kReload && valid) {
+      p0 = a.pin[2 * (size_t)i];
+      p1 = a.pin[2 * (size_t)i + 1];
     }
     if (soft && selfw != 0.0f) pt.x -= selfw * p0.w * rsqrtf(eps2);
 
