@@ -1571,15 +1571,19 @@ int gs_read_state(gs_ctx* ctx, float* particles8, float* stellar4) {
 int gs_write_state(gs_ctx* ctx, const float* particles8, const float* stellar4) {
   CTX_CHECK(ctx);
   SLOT(ctx, s);
-  for (int k = 0; k < 2; k++) {
-    if (particles8)
-      CK(ctx, cudaMemcpyAsync(ctx->part[k] + 2 * (size_t)s->off, particles8, (size_t)s->n * 32,
-                              cudaMemcpyHostToDevice, ctx->stream),
-         "state");
-    if (stellar4)
-      CK(ctx, cudaMemcpyAsync(ctx->stel[k] + s->off, stellar4, (size_t)s->n * 16, cudaMemcpyHostToDevice,
-                              ctx->stream),
-         "stellar");
+  // both ping-pong buffers get the records: one upload, then a device copy
+  float4* const p0 = ctx->part[0] + 2 * (size_t)s->off;
+  float4* const s0 = ctx->stel[0] + s->off;
+  if (particles8) {
+    CK(ctx, cudaMemcpyAsync(p0, particles8, (size_t)s->n * 32, cudaMemcpyHostToDevice, ctx->stream), "state");
+    CK(ctx, cudaMemcpyAsync(ctx->part[1] + 2 * (size_t)s->off, p0, (size_t)s->n * 32, cudaMemcpyDeviceToDevice,
+                            ctx->stream),
+       "state");
+  }
+  if (stellar4) {
+    CK(ctx, cudaMemcpyAsync(s0, stellar4, (size_t)s->n * 16, cudaMemcpyHostToDevice, ctx->stream), "stellar");
+    CK(ctx, cudaMemcpyAsync(ctx->stel[1] + s->off, s0, (size_t)s->n * 16, cudaMemcpyDeviceToDevice, ctx->stream),
+       "stellar");
   }
   return wait_stream(ctx, 0, s);
 }
