@@ -243,7 +243,14 @@ struct gs_ctx {
   int walk_split = 1;              // tuning: walk splits per work item of a lone galaxy (0: by its size; 1, 2, 4, 8)
   uint32_t walk_items[4] = {0, 0, 0, 0};  // work items per lanes-per-particle class (1, 2, 4, 8)
   bool walk_comp = false;  // Kahan-compensated far-field sums in the walk
-  void* host_stage = nullptr;  // pinned: [slots] params
+  // pinned staging of Params uploads: a ring of entries, each rewritten only after
+  // the copy that last read it has run (its event), so an update does not wait
+  // for the queued steps (NBodyGPU.updateParams is a queue write too)
+  static constexpr int kParamRing = 8;
+  void* host_stage = nullptr;  // pinned: [kParamRing] params
+  cudaEvent_t param_ev[kParamRing] = {};
+  bool param_used[kParamRing] = {};
+  int param_next = 0;
   // asynchronous position readback (gs_encode_position_readback), set up on first
   // use: a copy stream, the events ordering it after the compaction, a mapped
   // pinned word block for the diagnostics snapshot and the error word, and the
@@ -394,7 +401,9 @@ int pool_init(gs_ctx* c, int device, uint64_t cap, uint32_t slots) {
   CK(c, cudaMemset(c->diag_ctr, 0, sizeof(unsigned) * p.slots), "memset");
   CK(c, cudaMemset(c->partials, 0, sizeof(double) * kPartials * kWalkParts * p.groups), "memset");
   CK(c, cudaMemset(c->walk_work, 0, 16), "memset");
-  CK(c, cudaMallocHost(&c->host_stage, sizeof(gs_params) * (size_t)p.slots + 256), "pinned stage");
+  CK(c, cudaMallocHost(&c->host_stage, sizeof(gs_params) * (size_t)gs_ctx::kParamRing + 256), "pinned stage");
+  for (int k = 0; k < gs_ctx::kParamRing; k++)
+    CK(c, cudaEventCreateWithFlags(&c->param_ev[k], cudaEventDisableTiming), "params event");
   c->slots.assign(p.slots, Slot());
   c->palloc.init(p.cap);
   c->lay_dirty = true;
@@ -417,6 +426,11 @@ void pool_release(gs_ctx* c) {
   c->rb_stream = nullptr;
   c->rb_pending = false;
   if (c->host_stage) cudaFreeHost(c->host_stage);
+  for (int k = 0; k < gs_ctx::kParamRing; k++) {
+    if (c->param_ev[k]) cudaEventDestroy(c->param_ev[k]);
+    c->param_ev[k] = nullptr;
+    c->param_used[k] = false;
+  }
   if (c->ev) cudaEventDestroy(c->ev);
   if (c->stream) cudaStreamDestroy(c->stream);
   c->host_stage = nullptr;
@@ -1062,14 +1076,19 @@ int gs_update_params(gs_ctx* ctx, const gs_params* params) {
   if (!params) return ctx->fail(GS_EINVAL, "params is NULL");
   s->hp = *params;
   s->hp.N = s->n;
-  // the 96-byte uniform goes through pinned memory so the async copy never
-  // reads a caller buffer after return
-  gs_params* stage = reinterpret_cast<gs_params*>(ctx->host_stage) + ctx->sel;
-  CK(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+  // the 96-byte uniform goes through a pinned ring entry, so the async copy never
+  // reads the caller's buffer after return and the entry is free once its last
+  // copy has run
+  const int e = ctx->param_next;
+  ctx->param_next = (e + 1) % gs_ctx::kParamRing;
+  if (ctx->param_used[e]) CK(ctx, cudaEventSynchronize(ctx->param_ev[e]), "params stage");
+  gs_params* stage = reinterpret_cast<gs_params*>(ctx->host_stage) + e;
   *stage = s->hp;
   DevState* st = ctx->st + ctx->sel;
   CK(ctx, cudaMemcpyAsync(&st->p, stage, sizeof(gs_params), cudaMemcpyHostToDevice, ctx->stream),
      "params upload");
+  CK(ctx, cudaEventRecord(ctx->param_ev[e], ctx->stream), "params event");
+  ctx->param_used[e] = true;
   params_fixup_kernel<<<1, 1, 0, ctx->stream>>>(st, s->n);
   CK(ctx, cudaGetLastError(), "params fixup");
   return GS_OK;

@@ -96,7 +96,10 @@ int gs_create_on(int device, uint32_t N, const float* particles8, const float* s
                  gs_ctx** out);
 /* NBodyGPU.destroy (NBodyGPU.js:358-368). */
 int gs_destroy(gs_ctx* ctx);
-/* NBodyGPU.updateParams (NBodyGPU.js:253-275); N is forced to the context's N. */
+/* NBodyGPU.updateParams (NBodyGPU.js:253-275); N is forced to the context's N.
+ * Queued on the context's stream after the work already queued, without waiting
+ * for it (the reference's writeBuffer is a queue write too); params may be reused
+ * on return. */
 int gs_update_params(gs_ctx* ctx, const gs_params* params);
 /* Simulation clock (main.js simTime, a double): full steps stamp
  * Params.time = f32(simTime) and advance it by dt. gs_update_params sets it to
