@@ -11,6 +11,8 @@
   that FP32 and FP64 decide differently; reset returns and clears them.
 * gs_sync waits for queued work, bounded by a timeout; a wait that times out
   leaves the queued work and the context intact.
+* gs_update_params queues its copy without draining the stream; queued updates
+  and steps give what the same calls give one at a time.
 * The asynchronous position readback (gs_encode_position_readback /
   gs_await_position_readback) delivers the state of the step it followed while
   later steps run, one readback in flight at a time, with a bounded await.
@@ -190,3 +192,25 @@ def test_async_position_readback_timeout_and_python_mirror(gpu_lib):
     assert not _same(before, after) and np.all(np.isfinite(before))
     assert sim.readbackEnergy["mass"] > 0 and sim.deviceErrors() == 0
     sim.destroy()
+
+
+def test_params_updates_queue_without_waiting(gpu_lib):
+    """gs_update_params queues its copy behind the work already queued and does
+    not drain the stream (a ring of pinned staging entries, each reused only after
+    its copy has run). Twenty frames of [update with a new clock and theta, one full
+    step] queued without any wait, more frames than the ring has entries, end
+    bit-identical to the same frames run with a wait after each."""
+    g = ic.disk_16k()
+    runs = []
+    for wait in (False, True):
+        sim = NBodyGPU(0, g.particles, g.stellar)
+        for k in range(20):
+            sim.updateParams(dt=0.005, G=1.0, epsilon=0.05, theta=0.5 if k % 2 else 0.7, time=0.005 * k)
+            sim.run(1, False)
+            if wait:
+                sim.sync()
+        sim.sync()
+        runs.append(sim.readState())
+        assert sim.deviceErrors() == 0
+        sim.destroy()
+    assert _same(runs[0][0], runs[1][0]) and _same(runs[0][1], runs[1][1])
