@@ -327,8 +327,8 @@ def run_ours(args, ws, rank, local):
         sim.gpu.setWalkMode(False)
         sim.gpu.setComMode(0)
         precision["unit"] = "ms per full step, median of 20 (L2 flushed between steps)"
-        precision["modes"] = {"fp32": "FP32 walk, FP32 COM", "compensated": "Kahan far-field sums",
-                              "com64": "FP64 internal-node COM", "both": "Kahan sums + FP64 COM"}
+        precision["modes"] = {"fp32": "FP32 walk, FP32 COM", "compensated": "Kahan far-field sums per walk round",
+                              "com64": "FP64 internal-node COM", "both": "per-round Kahan sums + FP64 COM"}
 
     # ---- e2e through the C ABI with pinned host buffers ----
     e2e = None

@@ -242,7 +242,7 @@ struct gs_ctx {
   int walk_group = 32;             // tuning: walk group size (0: by galaxy size; 4, 8, 16 or 32 particles)
   int walk_split = 1;              // tuning: walk splits per work item of a lone galaxy (0: by its size; 1, 2, 4, 8)
   uint32_t walk_items[4] = {0, 0, 0, 0};  // work items per lanes-per-particle class (1, 2, 4, 8)
-  bool walk_comp = false;  // Kahan-compensated far-field sums in the walk
+  bool walk_comp = false;  // compensated far-field sums in the walk (a Kahan step per round)
   // pinned staging of Params uploads: a ring of entries, each rewritten only after
   // the copy that last read it has run (its event), so an update does not wait
   // for the queued steps (NBodyGPU.updateParams is a queue write too)

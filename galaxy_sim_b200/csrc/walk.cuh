@@ -309,8 +309,10 @@ __device__ __forceinline__ uint32_t warp_transpose(uint32_t x, int lane) {
 
 // ONE: the layout holds a single galaxy, whose descriptor comes with the
 // kernel parameters instead of a per-group lookup. COMP: far-field (monopole)
-// contributions are summed with Kahan compensation; near-field leaf sums add
-// plainly into the same sums.
+// contributions are accumulated with compensation, blocked by round: a round's
+// terms (at most 32 per lane) are summed plainly and each round's sum is added to
+// the particle's total with a Kahan step; near-field leaf sums add plainly into
+// the same totals.
 // MINB: resident blocks per SM the register budget is compiled for.
 // LPP: lanes per particle (walk group of 32 / LPP particles); a launch walks the
 // galaxies whose SegDesc wlpp field equals LPP and skips the others' work items.
@@ -489,6 +491,9 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
 #pragma unroll
       for (int r = 0; r < kWalkRanges; r++) th2[r] = (actbits >> r) & 1u ? theta2 : -INFINITY;
       uint32_t obits = 0;  // children this lane opens (active, not accepted), bit = slot
+      // COMP: the round's far-field terms (at most 32 per lane) are summed plainly,
+      // then the round's sum joins the particle's total in one Kahan step
+      float2 rax = f2(0.f), ray = f2(0.f), raz = f2(0.f), rpt = f2(0.f);
 #pragma unroll
       for (int kk = 0; kk < NPP; kk++) {
         // a range's pairs are tested only if the range was popped (one check per range)
@@ -515,16 +520,22 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
         const float2 mr = __fmul2_rn(qm, rinv);
         const float2 f = __fmul2_rn(__fmul2_rn(mr, rinv), rinv);
         if (COMP) {
-          kahan_add2(ax, cax, __fmul2_rn(rx, f));
-          kahan_add2(ay, cay, __fmul2_rn(ry, f));
-          kahan_add2(az, caz, __fmul2_rn(rz, f));
-          kahan_add2(pt, cpt, mr);
+          rax = __ffma2_rn(rx, f, rax);
+          ray = __ffma2_rn(ry, f, ray);
+          raz = __ffma2_rn(rz, f, raz);
+          rpt = __fadd2_rn(rpt, mr);
         } else {
           ax = __ffma2_rn(rx, f, ax);
           ay = __ffma2_rn(ry, f, ay);
           az = __ffma2_rn(rz, f, az);
           pt = __fadd2_rn(pt, mr);  // sum of m/r; potential = -G * sum
         }
+      }
+      if (COMP) {
+        kahan_add2(ax, cax, rax);
+        kahan_add2(ay, cay, ray);
+        kahan_add2(az, caz, raz);
+        kahan_add2(pt, cpt, rpt);
       }
       obits &= keep;
       const uint32_t om = __reduce_or_sync(full, obits);  // children opened by some lane

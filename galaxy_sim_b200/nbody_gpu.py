@@ -205,7 +205,7 @@ class NBodyGPU:
         self._ok(lib().gs_set_time(self._ctx, float(t)))
 
     def setWalkMode(self, compensated: bool):
-        """Kahan-compensated far-field sums in the walk (precision study)."""
+        """Compensated far-field sums in the walk, one Kahan step per walk round (precision study)."""
         self._ok(lib().gs_set_walk_mode(self._ctx, int(bool(compensated))))
 
     def setComMode(self, mode: int):

@@ -113,8 +113,10 @@ int gs_set_com_mode(gs_ctx* ctx, int mode);
  * galaxies with and without star formation share a pool. */
 int gs_set_star_formation(gs_ctx* ctx, int enable);
 /* Walk arithmetic: 0 = plain FP32 sums (default), 1 = far-field (monopole)
- * contributions summed with Kahan compensation. Together with gs_set_com_mode
- * this selects the precision variant; no counterpart in the reference. */
+ * contributions accumulated with compensation: each walk round's terms are
+ * summed plainly and the round's sum is added to the total with a Kahan step.
+ * Together with gs_set_com_mode this selects the precision variant; no
+ * counterpart in the reference. */
 int gs_set_walk_mode(gs_ctx* ctx, int compensated);
 /* Launch tuning (no counterpart in the reference). Takes effect at the next step;
  * galaxy_sim_b200/autotune.py picks values by timing.

@@ -3,7 +3,7 @@ holes with tracked halo centres, eps 0.02, theta 0.5, dt 0.005).
 
 Four arithmetic variants of the same step:
   * fp32        plain FP32 walk sums, FP32 COM cascade (refresh_level order),
-  * comp        Kahan-compensated far-field (monopole) sums, FP32 COM,
+  * comp        compensated far-field (monopole) sums (a Kahan step per walk round), FP32 COM,
   * fp32+com64  plain walk, FP32 leaves with FP64 internal-node COM sums,
   * comp+com64  both.
 Each is measured three ways: |da|/|a| against the FP64 walk of the same
