@@ -1,6 +1,7 @@
 // Stable LSD radix sort of 32-bit keys with a 32-bit payload, one kernel per
 // 8-bit digit ("onesweep": per-tile ranking by warp match, decoupled look-back
-// for the tile's digit offsets, direct scatter). A stable sort of
+// for the tile's digit offsets, scatter through shared memory so each digit's
+// run is written by consecutive threads). A stable sort of
 // (code, original index) gives exactly the permutation of radixSortIndices
 // (src/physics/mortonTree.js:68-84): ties keep their original order.
 //
@@ -66,10 +67,13 @@ __global__ void __launch_bounds__(kSortThreads)
                   uint32_t* lookback, uint32_t* tile_counter, Layout L, DevState* st,
                   uint32_t spin_limit = kSpinLimit, uint32_t withhold = kNoTile) {
   griddep_wait();  // launched with a programmatic dependency: predecessors' writes first
+  constexpr int kTileKeys = kSortThreads * ITEMS;
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kSortWarps][256];
-  __shared__ uint32_t s_prefix[256];
-  __shared__ uint32_t s_scan[kSortWarps];
+  __shared__ uint32_t s_prefix[256];  // global start of each digit's run, minus its tile-local start
+  __shared__ uint32_t s_local[256];   // tile-local start of each digit's run
+  __shared__ uint32_t s_scan[kSortWarps], s_tscan[kSortWarps];
+  __shared__ uint32_t s_key[kTileKeys], s_val[kTileKeys];  // the tile in output order
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int shift = 8 * pass;
   if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
@@ -82,7 +86,6 @@ __global__ void __launch_bounds__(kSortThreads)
   DevState* sst = st + sd.slot;
   const uint32_t lt = tile - sd.sort_tile0;  // tile index within the galaxy
   const uint32_t seg_end = sd.off + sd.n;
-  constexpr int kTileKeys = kSortThreads * ITEMS;
   const uint32_t base = sd.off + lt * kTileKeys + warp * (kTileKeys / kSortWarps);
 
   uint32_t key[ITEMS], val[ITEMS], rank[ITEMS];
@@ -121,18 +124,31 @@ __global__ void __launch_bounds__(kSortThreads)
     tot += c;
   }
   // The galaxy's exclusive offset of digit d (block-wide scan of its histogram).
+  // Also the tile-local start of digit d (a scan of the tile's own counts).
   const uint32_t h = hist[((size_t)sd.slot * kSortPasses + pass) * 256 + d];
-  uint32_t incl = h;
+  uint32_t incl = h, tincl = tot;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += t;
+    const uint32_t u = __shfl_up_sync(0xffffffffu, tincl, o);
+    if (lane >= o) {
+      incl += t;
+      tincl += u;
+    }
   }
-  if (lane == 31) s_scan[warp] = incl;
+  if (lane == 31) {
+    s_scan[warp] = incl;
+    s_tscan[warp] = tincl;
+  }
   __syncthreads();
-  uint32_t wpre = 0;
-  for (int w = 0; w < warp; w++) wpre += s_scan[w];
+  uint32_t wpre = 0, twpre = 0;
+  for (int w = 0; w < warp; w++) {
+    wpre += s_scan[w];
+    twpre += s_tscan[w];
+  }
   const uint32_t gexcl = sd.off + wpre + incl - h;
+  const uint32_t tlocal = twpre + tincl - tot;
+  s_local[d] = tlocal;
 
   uint32_t* lb = lookback + (size_t)tile * 256;
   const bool publish = tile != withhold;
@@ -175,22 +191,34 @@ __global__ void __launch_bounds__(kSortThreads)
     }
     if (publish) st_relaxed(&lb[d], kLbInc | ((excl + tot) & kLbMask));
   }
-  s_prefix[d] = excl;
+  s_prefix[d] = excl - tlocal;  // unsigned wrap: global position = local position + this
   __syncthreads();
 
+  // Scatter through shared memory: each key goes to its tile-local output position
+  // first, then consecutive threads write consecutive positions of each digit's
+  // run to global memory (the same positions as a direct scatter, coalesced).
 #pragma unroll
   for (int k = 0; k < ITEMS; k++) {
     if (base + k * 32 + lane < seg_end) {
       const uint32_t dd = (key[k] >> shift) & 255u;
-      const uint32_t pos = s_prefix[dd] + s_warp[warp][dd] + rank[k];
-      if (pos < sd.off || pos >= seg_end) {  // only after a failed look-back: flag, never write
-        raise_err(sst, GS_DERR_LOOKBACK);
-        continue;
-      }
-      keys_out[pos] = key[k];
-      vals_out[pos] = val[k];
-      if (LAST && inv_out) inv_out[val[k]] = pos;
+      const uint32_t lp = s_local[dd] + s_warp[warp][dd] + rank[k];
+      s_key[lp] = key[k];
+      s_val[lp] = val[k];
     }
+  }
+  __syncthreads();
+  const uint32_t tile_beg = sd.off + lt * kTileKeys;
+  const uint32_t nkeys = min((uint32_t)kTileKeys, seg_end - tile_beg);
+  for (uint32_t j = tid; j < nkeys; j += kSortThreads) {
+    const uint32_t kk = s_key[j], vv = s_val[j];
+    const uint32_t pos = j + s_prefix[(kk >> shift) & 255u];
+    if (pos < sd.off || pos >= seg_end) {  // only after a failed look-back: flag, never write
+      raise_err(sst, GS_DERR_LOOKBACK);
+      continue;
+    }
+    keys_out[pos] = kk;
+    vals_out[pos] = vv;
+    if (LAST && inv_out) inv_out[vv] = pos;
   }
 }
 
