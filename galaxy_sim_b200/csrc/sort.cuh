@@ -1,7 +1,7 @@
 // Stable LSD radix sort of 32-bit keys with a 32-bit payload, one kernel per
 // 8-bit digit ("onesweep": per-tile ranking by warp match, decoupled look-back
-// for the tile's digit offsets, scatter through shared memory so each digit's
-// run is written by consecutive threads). A stable sort of
+// for the tile's digit offsets; the passes before the last scatter through
+// shared memory so each digit's run is written by consecutive threads). A stable sort of
 // (code, original index) gives exactly the permutation of radixSortIndices
 // (src/physics/mortonTree.js:68-84): ties keep their original order.
 //
@@ -73,7 +73,11 @@ __global__ void __launch_bounds__(kSortThreads)
   __shared__ uint32_t s_prefix[256];  // global start of each digit's run, minus its tile-local start
   __shared__ uint32_t s_local[256];   // tile-local start of each digit's run
   __shared__ uint32_t s_scan[kSortWarps], s_tscan[kSortWarps];
-  __shared__ uint32_t s_key[kTileKeys], s_val[kTileKeys];  // the tile in output order
+  // the tile in output order (passes before the last; the last pass's digit, the
+  // code's top six bits, takes few values in a tile, so its runs are long and it
+  // scatters directly)
+  constexpr int kStage = LAST ? 1 : kTileKeys;
+  __shared__ uint32_t s_key[kStage], s_val[kStage];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int shift = 8 * pass;
   if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
@@ -194,31 +198,47 @@ __global__ void __launch_bounds__(kSortThreads)
   s_prefix[d] = excl - tlocal;  // unsigned wrap: global position = local position + this
   __syncthreads();
 
-  // Scatter through shared memory: each key goes to its tile-local output position
-  // first, then consecutive threads write consecutive positions of each digit's
-  // run to global memory (the same positions as a direct scatter, coalesced).
+  if (LAST) {  // direct scatter
 #pragma unroll
-  for (int k = 0; k < ITEMS; k++) {
-    if (base + k * 32 + lane < seg_end) {
-      const uint32_t dd = (key[k] >> shift) & 255u;
-      const uint32_t lp = s_local[dd] + s_warp[warp][dd] + rank[k];
-      s_key[lp] = key[k];
-      s_val[lp] = val[k];
+    for (int k = 0; k < ITEMS; k++) {
+      if (base + k * 32 + lane < seg_end) {
+        const uint32_t dd = (key[k] >> shift) & 255u;
+        const uint32_t pos = s_prefix[dd] + s_local[dd] + s_warp[warp][dd] + rank[k];
+        if (pos < sd.off || pos >= seg_end) {  // only after a failed look-back: flag, never write
+          raise_err(sst, GS_DERR_LOOKBACK);
+          continue;
+        }
+        keys_out[pos] = key[k];
+        vals_out[pos] = val[k];
+        if (inv_out) inv_out[val[k]] = pos;
+      }
     }
-  }
-  __syncthreads();
-  const uint32_t tile_beg = sd.off + lt * kTileKeys;
-  const uint32_t nkeys = min((uint32_t)kTileKeys, seg_end - tile_beg);
-  for (uint32_t j = tid; j < nkeys; j += kSortThreads) {
-    const uint32_t kk = s_key[j], vv = s_val[j];
-    const uint32_t pos = j + s_prefix[(kk >> shift) & 255u];
-    if (pos < sd.off || pos >= seg_end) {  // only after a failed look-back: flag, never write
-      raise_err(sst, GS_DERR_LOOKBACK);
-      continue;
+  } else {
+    // Scatter through shared memory: each key goes to its tile-local output
+    // position first, then consecutive threads write consecutive positions of each
+    // digit's run to global memory (the same positions as a direct scatter).
+#pragma unroll
+    for (int k = 0; k < ITEMS; k++) {
+      if (base + k * 32 + lane < seg_end) {
+        const uint32_t dd = (key[k] >> shift) & 255u;
+        const uint32_t lp = s_local[dd] + s_warp[warp][dd] + rank[k];
+        s_key[lp] = key[k];
+        s_val[lp] = val[k];
+      }
     }
-    keys_out[pos] = kk;
-    vals_out[pos] = vv;
-    if (LAST && inv_out) inv_out[vv] = pos;
+    __syncthreads();
+    const uint32_t tile_beg = sd.off + lt * kTileKeys;
+    const uint32_t nkeys = min((uint32_t)kTileKeys, seg_end - tile_beg);
+    for (uint32_t j = tid; j < nkeys; j += kSortThreads) {
+      const uint32_t kk = s_key[j], vv = s_val[j];
+      const uint32_t pos = j + s_prefix[(kk >> shift) & 255u];
+      if (pos < sd.off || pos >= seg_end) {  // only after a failed look-back: flag, never write
+        raise_err(sst, GS_DERR_LOOKBACK);
+        continue;
+      }
+      keys_out[pos] = kk;
+      vals_out[pos] = vv;
+    }
   }
 }
 
