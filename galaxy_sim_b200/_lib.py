@@ -96,6 +96,7 @@ SIGNATURES = [
     ("gs_morton_codes", _int, [_vp, _u32, _u32, _vp, _vp]),
     ("gs_radix_sort_indices", _int, [_vp, _u32, _vp]),
     ("gs_test_sort_lookback", _int, [_u32, _i64]),
+    ("gs_test_fail_alloc", _int, [_i64]),
     ("gs_tree_build", _int, [_vp, _vp, _vp, _u32, _f64, _u32, _vp, _vp, _vp, _u32, _vp]),
     ("gs_sort_and_build", _int, [_vp, _vp, _u32, _i64, _vp, _vp, _vp, _vp, _u32, _vp, _vp, _u32,
                                  _vp, _vp, _vp, _vp]),

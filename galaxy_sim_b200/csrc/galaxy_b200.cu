@@ -39,6 +39,9 @@ using namespace gs;
 namespace {
 
 thread_local char g_err[512] = "";
+// host-side fault injection (gs_test_fail_alloc): the number of device
+// allocations still to succeed before one fails; negative: none fails
+std::atomic<long long> g_fail_alloc_in{-1};
 
 constexpr uint64_t kMaxPool = 1ull << 27;  // node indices (2 cap + 4096) fit the walk's 29-bit fields
 constexpr uint32_t kMaxSlots = 4096;
@@ -285,6 +288,7 @@ struct gs_ctx {
   template <typename T>
   cudaError_t alloc(T** p, size_t count) {
     void* q = nullptr;
+    if (g_fail_alloc_in.load() >= 0 && g_fail_alloc_in.fetch_sub(1) == 0) return cudaErrorMemoryAllocation;
     cudaError_t e = cudaMalloc(&q, count * sizeof(T) + 16);
     if (e != cudaSuccess) return e;
     owned.push_back(q);
@@ -1879,6 +1883,15 @@ int gs_test_sort_lookback(uint32_t spin_limit, int64_t withhold_tile) {
   }
   g_test_spin_limit.store(spin_limit);
   g_test_withhold.store(withhold_tile < 0 ? kNoTile : (uint32_t)withhold_tile);
+  return GS_OK;
+}
+
+int gs_test_fail_alloc(int64_t nth) {
+  if (nth < -1) {
+    set_err(g_err, "nth must be an allocation count or -1");
+    return GS_EINVAL;
+  }
+  g_fail_alloc_in.store(nth);
   return GS_OK;
 }
 

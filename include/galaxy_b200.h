@@ -255,6 +255,12 @@ int gs_radix_sort_indices(const uint32_t* codes, uint32_t N, uint32_t* perm);
  * step graphs never use this setting. gs_test_sort_lookback(1u << 20, -1)
  * restores the production setting. */
 int gs_test_sort_lookback(uint32_t spin_limit, int64_t withhold_tile);
+/* Host-side fault injection for tests (no counterpart in the reference): after
+ * nth further device allocations made by the library's contexts, the next one
+ * fails as if the device were out of memory (it is reported as GS_ENOMEM and the
+ * call unwinds like a real failure); the switch then disarms itself. nth = -1
+ * disarms it. Nothing is injected on the device. */
+int gs_test_fail_alloc(int64_t nth);
 /* MortonTree.build (mortonTree.js:107-182) over sorted codes, stride-3 positions
  * and masses; max_nodes follows the MortonTree pool (2N + 4096 there). */
 int gs_tree_build(const uint32_t* sorted_codes, const float* pos3, const float* masses,
