@@ -12,7 +12,10 @@ With N > 1 (torchrun, one rank per GPU) every rank runs an independent replica
 (the path does not shard; there is no collective): weak scaling, value = all
 ranks' particle-steps / the slowest rank's device time.
 
-Timing: W untimed warm-up steps, then K steps, each bracketed by CUDA events on
+Timing: after the launch knobs are tuned, the galaxy goes back to its seeded
+initial conditions, so every timed leg covers the same early steps of the
+workload (the disk contracts, and later steps cost more interactions). Then W
+untimed warm-up steps, then K steps, each bracketed by CUDA events on
 the context's stream, with a 256 MiB L2 flush (2x the 126 MB L2) between steps;
 barrier + synchronize on both sides; max over ranks. ``e2e`` is the same
 metric through the C ABI with pinned host buffers, frame by frame as main.js
@@ -21,7 +24,8 @@ Params upload, the step and the position readback (16 B per particle, with the
 energy diagnostics of the same point) collected in the next frame as main.js
 collects its readback promise, and a final state readback, all inside the
 event-timed region. ``precision_modes`` gives the step time of the compensated
-walk and of the FP64 internal-node COM refresh on the same workload.
+walk and of the FP64 internal-node COM refresh on the same workload, each mode
+from the initial conditions.
 
 The same line carries the metric's batched and served halves (one GPU):
 ``batched`` = 96 disks (N log-uniform in [4096, 262144]) stepped as one pool,
@@ -206,6 +210,23 @@ def measured_peaks():
         return {}
 
 
+def restart(sim, g, w):
+    """Put a Simulation back at its galaxy's seeded initial conditions: particle
+    and stellar records, clock, Params and tracked centres, as Simulation sets
+    them up (the launch knobs stay)."""
+    from galaxy_sim_b200.simulation import params_dict
+
+    gpu = sim.gpu
+    gpu.writeState(g.particles, g.stellar)
+    gpu.setTime(0.0)
+    gpu.updateParams(**params_dict(g, w.physics))
+    c1, c2 = g.central
+    if c1 >= 0 or c2 >= 0:
+        hc = g.halo_centers
+        gpu.setTracking(c1, c2, hc[0] if len(hc) > 0 else None, hc[1] if len(hc) > 1 else None)
+    sim.sync()
+
+
 def run_ours(args, ws, rank, local):
     import numpy as np
     import torch
@@ -227,6 +248,11 @@ def run_ours(args, ws, rank, local):
     tuned = None
     if not args.no_tune:
         tuned = autotune(sim.gpu, steps=5, warmup=2, star_formation=sim.star_formation, device=local)
+        # the tuning steps advanced the galaxy (the disk contracts, so later steps
+        # cost more interactions): back to the seeded initial conditions, so the
+        # timed steps are steps W .. W + K of the workload, as in the e2e leg and
+        # the reference arm
+        restart(sim, g, w)
     sim.run(args.warmup)
     sim.sync()
     # kernels per step, counted from the captured step graph: bbox, codes, 4 sort
@@ -319,6 +345,7 @@ def run_ours(args, ws, rank, local):
     if not args.no_modes:
         precision = {}
         for name, comp, com in (("fp32", 0, 0), ("compensated", 1, 0), ("com64", 0, 2), ("both", 1, 2)):
+            restart(sim, g, w)  # every mode times the same steps of the workload
             sim.gpu.setWalkMode(bool(comp))
             sim.gpu.setComMode(com)
             sim.run(3)

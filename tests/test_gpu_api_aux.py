@@ -67,6 +67,38 @@ def test_checkpoint_restore_continues_bit_identical(gpu_lib):
     assert got_e == want_e
 
 
+def test_bench_restart_equals_a_fresh_start(gpu_lib):
+    """bench.py times its steps from the seeded initial conditions after tuning
+    the same context: its restart must leave nothing of the steps before."""
+    import os
+    import sys
+    from types import SimpleNamespace
+
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+
+    g = ic.two_galaxy_collision(20000, 7, gas_frac=0.3)
+    ph = Physics(0.02, 0.5, 0.005, gas_drag=0.25, sf_eff=0.05)
+    fresh = Simulation(g, ph)
+    fresh.run(3)
+    want_P, want_S = fresh.gpu.readState()
+    want_tr, want_e = fresh.gpu.getTracking(), fresh.gpu.energy()
+    fresh.close()
+
+    sim = Simulation(g, ph)
+    sim.run(6)
+    bench.restart(sim, g, SimpleNamespace(physics=ph))
+    sim.run(3)
+    got_P, got_S = sim.gpu.readState()
+    got_tr, got_e = sim.gpu.getTracking(), sim.gpu.energy()
+    assert sim.gpu.deviceErrors() == 0
+    sim.close()
+    assert _same(got_P, want_P) and _same(got_S, want_S)
+    assert got_tr[:2] == want_tr[:2]
+    assert np.array_equal(got_tr[2], want_tr[2]) and np.array_equal(got_tr[3], want_tr[3])
+    assert got_e == want_e
+
+
 def test_walk_counters_match_the_fp64_walk(gpu_lib, oracle):
     g = ic.disk_16k()
     sim = NBodyGPU(0, g.particles, g.stellar)
