@@ -111,3 +111,40 @@ def test_get_tree_on_a_pool_slot(gpu_lib):
     assert np.array_equal(lr, want_lr)
     assert np.array_equal(nodes.view(np.uint8), want_nodes.view(np.uint8))
     pool.close()
+
+
+def test_readmitted_pool_equals_a_fresh_pool(gpu_lib):
+    """bench.py times its pool from the seeded initial conditions after tuning it:
+    every galaxy removed, then admitted again in the same order. That must give
+    the same slots and the same results as a fresh pool."""
+    gals = []
+    for k, (n, gas) in enumerate(((3000, 0.3), (7000, 0.0), (1500, 0.3))):
+        g = ic.galaxy_disk(n, 50 + k, gas_frac=gas)
+        ph = Physics(0.02, 0.5, 0.005, gas_drag=0.25 if gas else 0.0, sf_eff=0.05 if gas else 0.0)
+        gals.append((g, ph))
+    cap = sum((g.N + 255) // 256 * 256 for g, _ in gals)
+
+    def admit(pool):
+        return [pool.add(g.particles, g.stellar, params_dict(g, ph), star_formation=ph.sf_eff > 0)
+                for g, ph in gals]
+
+    fresh = GalaxyPool(cap, len(gals))
+    want_slots = admit(fresh)
+    fresh.run(3, True)
+    want = [fresh.read_state(s) for s in want_slots]
+    want_e = fresh.energies()
+    fresh.close()
+
+    pool = GalaxyPool(cap, len(gals))
+    admit(pool)
+    pool.run(6, True)
+    for s in list(pool.n):
+        pool.remove(s)
+    slots = admit(pool)
+    assert slots == want_slots
+    pool.run(3, True)
+    for s, (wp, ws) in zip(slots, want):
+        gp, gs = pool.read_state(s)
+        assert _same(gp, wp) and _same(gs, ws), s
+    assert np.array_equal(pool.energies(), want_e)
+    pool.close()
