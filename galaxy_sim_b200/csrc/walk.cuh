@@ -180,6 +180,16 @@ struct WalkSmem {
 // force at r = 0) and its potential removed once at the end of the walk via
 // selfw (counted by the lane whose share holds it); otherwise it is skipped per
 // pair.
+// Reciprocal square root for the walk's r^2 + eps^2, which is never subnormal
+// (eps^2 is zero or at least the smallest normal float, and zero softening adds
+// that smallest normal instead): the flush-to-zero form gives the same result as
+// rsqrtf there and issues fewer instructions.
+__device__ __forceinline__ float rsqrt_walk(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 template <int LPP, typename Smem>
 __device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k, uint32_t kmax, uint32_t jself,
                                          bool me, bool soft, float2 px, float2 py, float2 pz,
@@ -198,7 +208,7 @@ __device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k
       const float2 jz = make_float2(jzm.x, jzm.y), jm = make_float2(jzm.z, jzm.w);
       const float2 ex = __fadd2_rn(jx, px), ey = __fadd2_rn(jy, py), ez = __fadd2_rn(jz, pz);
       const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __ffma2_rn(ez, ez, make_float2(e2me, e2me))));
-      const float2 ri = make_float2(rsqrtf(e2.x), rsqrtf(e2.y));
+      const float2 ri = make_float2(rsqrt_walk(e2.x), rsqrt_walk(e2.y));
       const float2 mr = __fmul2_rn(jm, ri);
       const float2 ff = __fmul2_rn(__fmul2_rn(mr, ri), ri);
       ax = __ffma2_rn(ex, ff, ax);
@@ -217,7 +227,7 @@ __device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k
       const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __ffma2_rn(ez, ez, make_float2(eps2, eps2))));
       const bool u0 = me && j < k && j != jself;
       const bool u1 = me && j + 1 < k && j + 1 != jself;
-      const float2 ri = make_float2(u0 ? rsqrtf(e2.x) : 0.0f, u1 ? rsqrtf(e2.y) : 0.0f);
+      const float2 ri = make_float2(u0 ? rsqrt_walk(e2.x) : 0.0f, u1 ? rsqrt_walk(e2.y) : 0.0f);
       const float2 mr = __fmul2_rn(jm, ri);
       const float2 ff = __fmul2_rn(__fmul2_rn(mr, ri), ri);
       ax = __ffma2_rn(ex, ff, ax);
@@ -260,12 +270,12 @@ __device__ __forceinline__ void leaf_batch(const Smem& S, uint32_t nbp, uint32_t
     if (SOFT) {
       const float e2me = me ? eps2 : INFINITY;
       const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __ffma2_rn(ez, ez, make_float2(e2me, e2me))));
-      ri = make_float2(rsqrtf(e2.x), rsqrtf(e2.y));
+      ri = make_float2(rsqrt_walk(e2.x), rsqrt_walk(e2.y));
     } else {
       const uint32_t j2 = 2 * (sub + LPP * kk);  // the pair's first source in the batch
       const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __ffma2_rn(ez, ez, make_float2(eps2, eps2))));
-      ri = make_float2(me && j2 != selfloc ? rsqrtf(e2.x) : 0.0f,
-                       me && j2 + 1 != selfloc ? rsqrtf(e2.y) : 0.0f);
+      ri = make_float2(me && j2 != selfloc ? rsqrt_walk(e2.x) : 0.0f,
+                       me && j2 + 1 != selfloc ? rsqrt_walk(e2.y) : 0.0f);
     }
     const float2 mr = __fmul2_rn(jm, ri);
     const float2 ff = __fmul2_rn(__fmul2_rn(mr, ri), ri);
@@ -354,7 +364,11 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
     const float eps2p = __ldg(&P.epsilon2);
     const float theta2 = __ldg(&P.theta) * __ldg(&P.theta);
     const float qe2 = 0.25f * eps2p;
-    const bool soft = eps2p > 0.0f;  // self pairs may then be summed and removed afterwards
+    // Self pairs may be summed and removed afterwards when softened. Softening below
+    // the smallest normal float counts as none, so every r^2 + eps^2 below is a
+    // normal number (or +inf, or NaN from non-finite input), for which the
+    // flush-to-zero rsqrt gives the same result as the non-flushing one.
+    const bool soft = eps2p >= 1.17549435e-38f;
     // Without softening a node test at r = 0 (a particle's own one-particle leaf)
     // would weigh rsqrt(0) = inf by 0 (NaN): the distances add the smallest
     // normal float instead, which moves no r^2 above 1e-30 by more than a
@@ -516,7 +530,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) walk_kernel(WalkArgs a) {
         obits |= (~ax_ & (1u << c)) | (~ay_ & (2u << c));
         const float2 dsel = make_float2(__uint_as_float((__float_as_uint(d2.x) & ax_) | (0x7f800000u & ~ax_)),
                                         __uint_as_float((__float_as_uint(d2.y) & ay_) | (0x7f800000u & ~ay_)));
-        const float2 rinv = make_float2(rsqrtf(dsel.x), rsqrtf(dsel.y));
+        const float2 rinv = make_float2(rsqrt_walk(dsel.x), rsqrt_walk(dsel.y));
         const float2 mr = __fmul2_rn(qm, rinv);
         const float2 f = __fmul2_rn(__fmul2_rn(mr, rinv), rinv);
         if (COMP) {
