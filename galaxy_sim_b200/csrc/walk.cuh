@@ -176,7 +176,7 @@ struct WalkSmem {
 // (nbody_bh.wgsl:117-131), used by walk groups of 32: two sources per packed
 // step, up to kmax >= k (staged sources past a leaf's count are massless zeros).
 // A particle served by LPP lanes splits the source pairs: lane `sub` takes pairs
-// sub, sub + LPP, ... With soft (eps^2 > 0) the self pair is included (zero
+// sub, sub + LPP, ... With soft (eps^2 a normal float) the self pair is included (zero
 // force at r = 0) and its potential removed once at the end of the walk via
 // selfw (counted by the lane whose share holds it); otherwise it is skipped per
 // pair.
@@ -245,7 +245,7 @@ __device__ __forceinline__ void leaf_sum(const Smem& S, uint32_t off, uint32_t k
 // massless zero). A particle served by LPP lanes splits the pairs: lane `sub`
 // takes pairs sub, sub + LPP, ... Bit LPP * kk of `pm` tells whether the
 // particle opened the leaf of pair sub + LPP * kk.
-// With soft (eps^2 > 0) a pair the lane does not take gets eps^2 = +inf: r^2 +
+// With soft (eps^2 a normal float) a pair the lane does not take gets eps^2 = +inf: r^2 +
 // eps^2 is then +inf, rsqrt gives 0 and every term vanishes (r is finite); the
 // self pair is included (zero force at r = 0) and its potential removed once at
 // the end of the walk. Without softening the self pair (batch source `selfloc`)
