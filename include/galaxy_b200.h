@@ -51,7 +51,9 @@ extern "C" {
 
 typedef struct gs_ctx gs_ctx;
 
-/* 96-byte Params uniform (nbody_bh.wgsl:19-42). */
+/* 96-byte Params uniform (nbody_bh.wgsl:19-42). epsilon2 below the smallest
+ * normal float (1.17549435e-38) is walked as no softening: each particle's own
+ * pair is then skipped instead of summed. */
 typedef struct gs_params {
   float dt, G, epsilon2;
   uint32_t N;
