@@ -47,6 +47,22 @@ def test_library_reports_errors_without_gpu():
     assert L.gs_step(None) == _lib.GS_EINVAL
 
 
+def test_fault_injection_settings_check_their_arguments_without_gpu():
+    """The host-side failure-detection settings are armed and disarmed on the
+    host alone, and refuse values that mean nothing."""
+    from galaxy_sim_b200 import _lib
+
+    L = _lib.lib()
+    assert L.gs_test_fail_alloc(-2) == _lib.GS_EINVAL
+    assert b"allocation count or -1" in L.gs_last_error(None)
+    assert L.gs_test_fail_alloc(7) == _lib.GS_OK
+    assert L.gs_test_fail_alloc(-1) == _lib.GS_OK
+    assert L.gs_test_sort_lookback(0, -1) == _lib.GS_EINVAL
+    assert b"spin_limit must be positive" in L.gs_last_error(None)
+    assert L.gs_test_sort_lookback(1 << 20, -2) == _lib.GS_EINVAL
+    assert L.gs_test_sort_lookback(1 << 20, -1) == _lib.GS_OK
+
+
 def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     from galaxy_sim_b200 import _lib
 
