@@ -209,3 +209,22 @@ def test_sort_lookback_wait_runs_out_and_reports(gpu_lib, oracle):
     assert b"0x1" in L.gs_last_error(None)
     assert L.gs_radix_sort_indices(codes.ctypes.data, codes.size, perm.ctypes.data) == 0
     assert np.array_equal(perm, want)
+
+
+def test_subnormal_softening_walks_as_none(gpu_lib):
+    """epsilon2 below the smallest normal float is walked as no softening (every
+    reciprocal square root the walk takes stays a normal number): the steps equal
+    those at epsilon = 0 bit for bit and stay finite."""
+    g = ic.disk_16k()
+    assert 0.0 < np.float32(1e-20 * 1e-20) < np.finfo(np.float32).tiny
+    out = []
+    for eps in (0.0, 1e-20):
+        sim = NBodyGPU(0, g.particles, g.stellar)
+        sim.updateParams(dt=0.005, G=1.0, epsilon=eps, theta=0.5)
+        sim.run(2, False)
+        P, _ = sim.readState()
+        assert sim.deviceErrors() == 0
+        sim.destroy()
+        out.append(P)
+    assert np.all(np.isfinite(out[0]))
+    assert np.array_equal(out[0].view(np.uint32), out[1].view(np.uint32))
